@@ -1,0 +1,342 @@
+#!/usr/bin/env python
+"""Model G stepper throughput on B200: site-updates/s and % of the HBM roofline.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--N 256]
+
+Workload: the full Model G step "PV2HBSplit23" (3 x [ideal PV2(dt/3) + 2 x phi
+heat bath(dt/6)] + charge heat bath(dt), Stepper.cxx:542-580) on a 256^3
+periodic FP64 lattice with the config-1 coefficients at H = 0.003 (m^2 = -4.813,
+lambda = 10, Gamma = 1, chi = 5, D = 1/3, dt = 0.04), measuring every 10 steps
+(saveFrequency, SuperPions.cxx:127-140).  Seeded synthetic state: phi ~
+0.1 N(0,1), charges ~ sqrt(chi) N(0,1) with the zero mode removed.  The state
+(1.34 GB) is larger than L2, so no flush is needed between steps.
+
+One process per GPU; for N > 1 each rank advances its own replica (distinct
+seed): the stepper does not shard, so scaling is weak, with no data-path
+collective.  Rank 0 prints one JSON line.
+
+--impl reference times the reference algorithm on the host cores: the CPU
+restatement in oracle/ (the reference itself needs PETSc/MPI/HDF5/FFTW, absent
+here), drawing from the reference's own serial xoroshiro128+ stream, with one
+thread per emulated MPI rank on a bounded lattice sample.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+ALG_BYTES = {  # algorithmic bytes per site, per launch (each input read once, each output written once)
+    "ideal": 160.0,    # 10 doubles in, 10 out
+    "phi_hb": 32.0,    # one parity pass: 64 B/site per full sweep, half the sites per launch
+    "charge": 96.0,    # one (direction, parity) face: 6 charges in and out for every site
+    "em": 64.0,
+}
+STEP_BYTES = {"PV2HBSplit23": 1440.0, "PV2HBSplit11": 800.0}
+KCLASS = {"ideal": 0, "phi_hb": 1, "charge": 2, "em": 3, "measure": 4}
+COEF = dict(mass0=-4.813, lam=10.0, H=0.003, chi=5.0, gamma=1.0, diffusion=1.0 / 3.0)
+DT = 0.04
+MEASURE_EVERY = 10
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--N", type=int, default=256)
+    ap.add_argument("--scounts", default="2,3")
+    ap.add_argument("--seed", type=int, default=122335456)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_table():
+    p = os.path.join(REPO, "profiles", "traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return {}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(index), f"--query-gpu={self.Q}", "--format=csv,noheader",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        self.p.wait()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        mhz, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                mhz.append(float(r[1].split()[0]))
+                mx = float(r[2].split()[0])
+            except (ValueError, IndexError):
+                continue
+            for n, v in zip(names, r[5:9]):
+                if "Active" in v and "Not" not in v:
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(mhz) if mhz else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(mhz)}
+
+
+def cpu_reference_rate(N, scounts, seconds=15.0, steps=None, warmup=1):
+    """The reference algorithm on the host cores (oracle port, reference RNG)."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import numpy as np
+    import oracle
+
+    cores = os.cpu_count() or 1
+    R = max(1, min(cores, N))
+    o = oracle.Oracle(N, mode=oracle.SEQUENTIAL, nranks=R, seed=122335456, **COEF)
+    o.initialize(1, 0.1)
+    o.initialize(2)
+    for _ in range(warmup):
+        o.step(0, DT, inner=scounts[0], outer=scounts[1])
+    done, t0 = 0, time.perf_counter()
+    while True:
+        o.step(0, DT, inner=scounts[0], outer=scounts[1])
+        done += 1
+        el = time.perf_counter() - t0
+        if (steps is not None and done >= steps) or (steps is None and el >= seconds):
+            break
+    return N ** 3 * done / el, R, done, el
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    scounts = tuple(int(x) for x in a.scounts.split(","))
+    name = "PV2HBSplit%d%d" % scounts
+    cores = os.cpu_count() or 1
+    Ns = 128 if cores >= 16 else 64
+    rate, R, done, el = cpu_reference_rate(Ns, scounts, steps=a.steps, warmup=a.warmup)
+    sample = (f"{done} timed steps (+{a.warmup} warm-up) of {name} on a {Ns}^3 sample lattice of the "
+              f"{a.N}^3 workload, {R} threads = emulated MPI z-slab ranks, reference serial RNG")
+    line = {
+        "impl": "reference", "metric": "Model G site-updates/s", "value": rate, "unit": "site-updates/s",
+        "n_gpus": a.gpus, "steps": done, "warmup": a.warmup, "ms_per_step": el / done * 1e3 * (a.N / Ns) ** 3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"Model G {name}, {a.N}^3 periodic, FP64 (CPU on a {Ns}^3 sample)", "N": a.N,
+                   "sample_N": Ns, "dt": DT, **COEF},
+        "cpu_baseline": {"value": rate, "unit": "site-updates/s", "cores": R, "kind": "port", "sample": sample},
+        "e2e": {"value": rate, "unit": "site-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def run_ours(a):
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    from langevina_b200 import _lib as L
+
+    lib = L.load()
+    scounts = tuple(int(x) for x in a.scounts.split(","))
+    name = "PV2HBSplit%d%d" % scounts
+    N = a.N
+    V = N ** 3
+    p = L.make_params(N, seed=a.seed + rank, **COEF)
+    h = C.c_void_p()
+    L.check(lib.lgv_create(C.byref(p), C.byref(h)), "lgv_create")
+    stream = torch.cuda.Stream()
+    L.check(lib.lgv_set_stream(h, C.c_void_p(stream.cuda_stream)), "lgv_set_stream")
+    L.check(lib.lgv_initialize(h, L.INIT_PHI_GAUSSIAN, 0.1), "init phi")
+    L.check(lib.lgv_initialize(h, L.INIT_CHARGES_GAUSSIAN, 0.0), "init charges")
+    msize = lib.lgv_measure_size(N)
+    meas = torch.empty(msize, dtype=torch.float64, device="cuda")
+
+    t_sim = 0.0
+
+    def one_step(s):
+        nonlocal t_sim
+        if s % MEASURE_EVERY == 0:
+            L.check(lib.lgv_measure_device(h, C.c_void_p(meas.data_ptr())), "measure")
+        L.check(lib.lgv_step(h, L.PV2HBSPLIT, scounts[0], scounts[1], DT, t_sim, 1), "step")
+        t_sim += DT
+
+    for s in range(a.warmup):
+        one_step(s)
+    torch.cuda.synchronize()
+
+    # ---- timed region: device-resident state ---------------------------------
+    L.check(lib.lgv_timing_enable(h, 1), "timing")
+    clocks = ClockSampler(local)
+    time.sleep(0.3)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for s in range(a.steps):
+        one_step(s)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ck = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    kern = {}
+    for k, c in KCLASS.items():
+        tot, n = C.c_double(), C.c_int64()
+        L.check(lib.lgv_timing_read(h, c, C.byref(tot), C.byref(n)), "timing_read")
+        kern[k] = (tot.value, n.value)
+    L.check(lib.lgv_timing_enable(h, 0), "timing off")
+    n_meas = len(range(0, a.steps, MEASURE_EVERY))
+    launches = 0
+    for k, (tot, n) in kern.items():
+        launches += n * (5 if k == "measure" else 1)
+
+    value = V * a.steps * world / (ms / 1e3)
+    peak, peak_kind = peaks()
+    dom = max((k for k in ALG_BYTES if kern[k][1] > 0), key=lambda k: kern[k][0])
+    tot, n = kern[dom]
+    avg_ms = tot / n
+    alg = ALG_BYTES[dom] * V
+    achieved = alg / (avg_ms / 1e3) / 1e9
+    trow = traffic_table().get(dom)
+    traffic = None
+    if trow:
+        traffic = trow["bytes_per_site"] * V
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
+                if peak_kind == "measured" else "fallback 6.65 TB/s",
+                "traffic": traffic, "alg_bytes_per_launch": alg, "avg_launch_ms": avg_ms}
+    kernels = {k: {"launches": kern[k][1], "total_ms": kern[k][0],
+                   "avg_ms": (kern[k][0] / kern[k][1]) if kern[k][1] else None,
+                   "alg_GBps": (ALG_BYTES[k] * V / (kern[k][0] / kern[k][1] / 1e3) / 1e9)
+                   if (k in ALG_BYTES and kern[k][1]) else None}
+               for k in kern}
+    step_frac = STEP_BYTES.get(name, float("nan")) * V * a.steps * 1.0 / (ms / 1e3) / 1e9 / peak
+
+    # ---- e2e: through the C ABI with host buffers -----------------------------
+    e2e = None
+    if not a.no_e2e:
+        u_host = torch.empty(V * 10, dtype=torch.float64).pin_memory()
+        meas_host = L.Measurement(N)
+        ms_struct = meas_host.struct()
+        L.check(lib.lgv_get_state(h, C.c_void_p(u_host.data_ptr())), "get_state")
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        L.check(lib.lgv_set_state(h, C.c_void_p(u_host.data_ptr())), "set_state")
+        ts = 0.0
+        for s in range(a.steps):
+            if s % MEASURE_EVERY == 0:
+                L.check(lib.lgv_measure(h, C.byref(ms_struct)), "measure")
+            L.check(lib.lgv_step(h, L.PV2HBSPLIT, scounts[0], scounts[1], DT, ts, 1), "step")
+            ts += DT
+        L.check(lib.lgv_get_state(h, C.c_void_p(u_host.data_ptr())), "get_state")
+        el = time.perf_counter() - t0
+        if dist:
+            t = torch.tensor([el], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            el = float(t.item())
+        mbytes = msize * 8
+        e2e = {"value": V * a.steps * world / el, "unit": "site-updates/s",
+               "h2d_bytes_per_step": 80 * V / a.steps,
+               "d2h_bytes_per_step": (80 * V + n_meas * mbytes) / a.steps,
+               "what": "lgv_set_state from pinned host AoS, K x lgv_step with lgv_measure to host every 10 steps, "
+                       "lgv_get_state back to pinned host AoS; host wall clock"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        rate, R, done, el = cpu_reference_rate(128 if (os.cpu_count() or 1) >= 16 else 64, scounts, seconds=12.0)
+        Ns = 128 if (os.cpu_count() or 1) >= 16 else 64
+        cpu = {"value": rate, "unit": "site-updates/s", "cores": R, "kind": "port",
+               "sample": f"{done} {name} steps on a {Ns}^3 sample lattice ({el:.1f} s), oracle port with the "
+                         f"reference serial RNG, one thread per emulated MPI rank"}
+
+    lgv_destroy = lib.lgv_destroy
+    lgv_destroy(h)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {
+        "metric": "Model G site-updates/s", "value": value, "unit": "site-updates/s", "n_gpus": world,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"Model G {name}, {N}^3 periodic lattice, FP64, measure every {MEASURE_EVERY} steps",
+                   "N": N, "evolver": name, "dt": DT, **COEF, "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (state 1.34 GB at 256^3), no flush"},
+        "roofline": roofline,
+        "step_hbm_frac": step_frac,
+        "step_alg_bytes_per_site": STEP_BYTES.get(name),
+        "kernels": kernels,
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": launches,
+        "clocks": ck,
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        return run_reference(a)
+    return run_ours(a)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

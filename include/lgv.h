@@ -1,0 +1,223 @@
+/*
+ * lgv.h -- C ABI of the B200 (sm_100a) Model A / Model G stepper and measurer.
+ *
+ * This is the drop-in boundary for the time stepper of langevinA
+ * (derek-teaney/langevinA, directory ModelG/).  Every entry point below names the
+ * reference interface it replaces.  Signatures use plain C types only: no CUDA,
+ * PETSc or torch types cross this boundary, so the library can be bound from C,
+ * C++ (see langevina.hpp), Python ctypes or any other FFI.
+ *
+ * Conventions
+ *  - Every function returns an int status: LGV_OK (0) or a negative LGV_ERR_*.
+ *    lgv_status_string() turns it into text; lgv_last_error() gives the detail
+ *    of the last failure on the calling thread.
+ *  - A handle owns one periodic N^3 lattice on the current CUDA device.  It is
+ *    not thread safe: use one handle per host thread.
+ *  - Host state arrays use the reference's site layout (G_node / data_node,
+ *    ModelA.h:274-286) in DMDA natural ordering u[k][j][i][L], L = 0..9 =
+ *    (phi_0..phi_3, A_1..A_3, V_1..V_3), FP64, 80 bytes per site.
+ *  - All arithmetic is FP64.
+ */
+#ifndef LGV_H
+#define LGV_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LGV_NPHI 4
+#define LGV_NA 3
+#define LGV_NV 3
+#define LGV_NDOF 10
+#define LGV_NOBS 11       /* Measurer::NObs, measurer.h:91-92 */
+#define LGV_NOBS_PHASE 14 /* Measurer::NObsPhase = NObsRotated, measurer.h:111,119 */
+
+/* Status codes. */
+#define LGV_OK 0
+#define LGV_ERR_INVALID (-1)     /* bad argument (size, pointer, enum) */
+#define LGV_ERR_CUDA (-2)        /* a CUDA runtime call failed */
+#define LGV_ERR_NOMEM (-3)       /* device or host allocation failed */
+#define LGV_ERR_TIMEOUT (-4)     /* a bounded device wait gave up */
+#define LGV_ERR_STATE (-5)       /* call not valid now (e.g. injected noise not supplied) */
+#define LGV_ERR_UNSUPPORTED (-6) /* valid request this build does not implement */
+
+/* Model parameters.  Replaces ModelAData / ModelACoefficients (ModelA.h:71-111,
+ * 185-248); the JSON keys of the same names are read by langevina.hpp. */
+typedef struct lgv_params {
+  int32_t N;         /* NX = NY = NZ; even and >= 4 (checkerboard) */
+  int32_t reserved0; /* must be 0 */
+  double LX;         /* box length, lattice spacing hX = LX / N (ModelA.h:199) */
+  double mass0;      /* m^2(t) = mass0 + dmassdt * t (ModelA.h:84) */
+  double dmassdt;
+  double lambda;
+  double H;
+  double chi;
+  double gamma;
+  double diffusion; /* sigma = diffusion * chi (ModelA.h:86) */
+  uint64_t seed;    /* base seed of the counter-based noise */
+} lgv_params;
+
+/* Steppers.  PV2HBSplit is the composer of Stepper.cxx:537-580; with
+ * (inner, outer) = (2, 3) it is the reference's "PV2HBSplit23". */
+#define LGV_PV2HBSPLIT 0             /* (A B^inner)^outer C */
+#define LGV_PV2HBSPLIT_NODIFFUSE 1   /* (A B^inner)^outer       */
+#define LGV_PV2HBSPLIT_ONLYDIFFUSE 2 /*                      C  */
+#define LGV_IDEAL_PV2 3              /* A : IdealPV2 (no accept/reject) */
+#define LGV_EULER_LANGEVIN_HB 4      /* B : phi checkerboard heat bath */
+#define LGV_CHARGE_HB 5              /* C : link charge heat bath */
+#define LGV_MODELA_EM 6              /* Euler-Maruyama Model A relaxation */
+
+/* Noise sources. */
+#define LGV_NOISE_COUNTER 0  /* counter-indexed xoroshiro128+ streams (production) */
+#define LGV_NOISE_INJECTED 1 /* caller-supplied uniforms / normals (parity tests) */
+
+/* lgv_initialize() kinds. */
+#define LGV_INIT_ZERO 0             /* ModelA::initialize() without a function */
+#define LGV_INIT_PHI_GAUSSIAN 1     /* phi_a ~ scale * N(0,1), charges untouched */
+#define LGV_INIT_CHARGES_GAUSSIAN 2 /* n ~ sqrt(chi) N(0,1), zero mode removed */
+
+/* Monitors (o4_stepper_monitor, Stepper.h:17-49). */
+#define LGV_MONITOR_IDEAL 0
+#define LGV_MONITOR_PHI_HB 1
+#define LGV_MONITOR_CHARGE_HB 2
+
+typedef struct lgv_monitor {
+  int64_t down_counts; /* dS < 0 */
+  int64_t up_counts;   /* dS >= 0 */
+  int64_t up_yes;      /* accepted with dS >= 0 */
+  int64_t up_no;       /* rejected */
+  double down_dS;      /* sum of dS over dS < 0 */
+  double up_dS;        /* sum of dS over accepted dS >= 0 */
+} lgv_monitor;
+
+/* Measurement output, caller-owned.  Any pointer may be NULL to skip that
+ * output.  Layouts follow Measurer (measurer.h:88-128) row-major:
+ *   OAverage            [11]
+ *   wall[a]             [11][N]            a = 0,1,2 for X,Y,Z
+ *   wall_k[a]           [11][N/2+1][2]     (re, im)
+ *   wall_k_rotated[a]   [14][N/2+1][2]
+ *   wall_phase[a]       [14][N]
+ *   wall_phase_k[a]     [14][N/2+1][2]                                      */
+typedef struct lgv_measurement {
+  double *OAverage;
+  double *wall[3];
+  double *wall_k[3];
+  double *wall_k_rotated[3];
+  double *wall_phase[3];
+  double *wall_phase_k[3];
+} lgv_measurement;
+
+typedef struct lgv_handle lgv_handle;
+
+/* Library identification. */
+int lgv_version(void);
+const char *lgv_status_string(int status);
+const char *lgv_last_error(void);
+
+/* Replaces: ModelA::ModelA (ModelA.h:311-336) -- DMDACreate3d + Vec + seeding.
+ * Allocates the device lattice on the current CUDA device. */
+int lgv_create(const lgv_params *params, lgv_handle **out);
+/* Replaces: ModelA::finalize / Stepper::finalize resource release
+ * (ModelA.h:338-352, Stepper.cxx:270-279,390-398,524-533). */
+int lgv_destroy(lgv_handle *h);
+/* Update coefficients (mass0, lambda, H, chi, gamma, diffusion, dmassdt, LX,
+ * seed) without reallocating; N must match. */
+int lgv_set_params(lgv_handle *h, const lgv_params *params);
+
+/* Replaces: VecLoad / direct writes into model->solution (ModelA.h:356-380,
+ * 443-458).  host_aos holds N^3 * 10 doubles in u[k][j][i][L] order. */
+int lgv_set_state(lgv_handle *h, const double *host_aos);
+/* Replaces: reads of model->solution (DMDAVecGetArray, VecView ModelA.h:384-402). */
+int lgv_get_state(lgv_handle *h, double *host_aos);
+/* Same two calls with a device pointer to an AoS array on the handle's device. */
+int lgv_set_state_device(lgv_handle *h, const double *dev_aos);
+int lgv_get_state_device(lgv_handle *h, double *dev_aos);
+
+/* Replaces: ModelA::initialize (ModelA.h:408-461, zero start) and
+ * ModelA::initialize_gaussian_charges (ModelA.h:463-525).  Noise comes from
+ * the counter streams (one counter value per call). */
+int lgv_initialize(lgv_handle *h, int kind, double scale);
+
+/* Noise control.  Replaces the global ModelARndm (NoiseGenerator.h:62-160) for
+ * the device-side draws.  The counter is the 64-bit sub-step index of the
+ * counter streams; saving (seed, counter) replaces the <tag>_<rank>.rng file
+ * (NoiseGenerator.h:112-146). */
+int lgv_set_noise_mode(lgv_handle *h, int mode);
+int lgv_set_counter(lgv_handle *h, uint64_t counter);
+int lgv_get_counter(lgv_handle *h, uint64_t *counter);
+/* Injected noise for the next sub-step of each kind (host pointers, copied).
+ *  hb:     prop[4][V] proposals in (-sqrt3, sqrt3) (variance1()), acc[V] in [0,1)
+ *          indexed by natural site index n = (k*N + j)*N + i.
+ *  charge: order[5] = (orderxyz[3], ordereo[2]) as after std::shuffle
+ *          (Stepper.cxx:461-466); q[6][6][V], acc[6][6][V] indexed by
+ *          (pass, L-4, natural index of the A site).
+ *  em:     xi[4][V] standard normals. */
+int lgv_inject_hb(lgv_handle *h, const double *prop, const double *acc);
+int lgv_inject_charge(lgv_handle *h, const int32_t *order, const double *q, const double *acc);
+int lgv_inject_em(lgv_handle *h, const double *xi);
+
+/* Replaces: Stepper::step(dt) (Stepper.h:6-11) for every stepper of
+ * Stepper.cxx (IdealPV2::step :23-66, EulerLangevinHB::step :287-389,
+ * ModelGChargeHB::step :449-522, PV2HBSplit::step :542-580) plus the
+ * Euler-Maruyama Model A step.  Runs nsteps steps of size dt starting at time
+ * t (t advances by dt per step; it sets m^2(t)).  inner/outer are the
+ * PV2HBSplit scounts {inner, outer} (ignored by the other evolvers).
+ * Asynchronous on the handle's stream. */
+int lgv_step(lgv_handle *h, int evolver, int inner, int outer, double dt, double t, int nsteps);
+
+/* Replaces: Measurer::measure(Vec*) (measurer.h:169-179, measurer.cxx:10-317):
+ * wall sums, phase walls, OAverage, x->k modes (FFTW r2c / N) and rotate_to_vev.
+ * Synchronous: the outputs are filled when it returns. */
+int lgv_measure(lgv_handle *h, lgv_measurement *out);
+/* Same measurement, left in device memory: dev_out receives
+ * lgv_measure_size(N) doubles packed in the order of lgv_measurement's fields
+ * (OAverage, wall[0..2], wall_k[0..2], wall_k_rotated[0..2], wall_phase[0..2],
+ * wall_phase_k[0..2]).  Asynchronous. */
+int lgv_measure_device(lgv_handle *h, double *dev_out);
+size_t lgv_measure_size(int N);
+
+/* Replaces: IdealPV2::computeEnergy (Stepper.cxx:204-268).  Synchronous. */
+int lgv_energy(lgv_handle *h, double *energy);
+
+/* Replaces: o4_stepper_monitor counters (Stepper.h:17-83).  Counting is off
+ * by default (it costs one block reduction per launch); lgv_enable_monitors
+ * turns it on and zeroes the counters. */
+int lgv_enable_monitors(lgv_handle *h, int enable);
+int lgv_get_monitor(lgv_handle *h, int which, lgv_monitor *out);
+
+/* Stream control: all work of the handle is issued on this cudaStream_t
+ * (NULL = the legacy default stream). */
+int lgv_set_stream(lgv_handle *h, void *cuda_stream);
+int lgv_synchronize(lgv_handle *h);
+
+/* Live kernel timing.  When enabled, every kernel launch of the classes below
+ * is bracketed by a CUDA event pair on the handle's stream; lgv_timing_read
+ * synchronizes, adds the elapsed times of all pairs recorded so far and
+ * returns the running total and launch count of one class.  Enabling (or
+ * re-enabling) resets the totals.  A "launch" of LGV_KCLASS_PHI_HB is one
+ * checkerboard parity pass; of LGV_KCLASS_CHARGE one (direction, parity) face;
+ * of LGV_KCLASS_MEASURE one full measurement (five small kernels). */
+#define LGV_KCLASS_IDEAL 0
+#define LGV_KCLASS_PHI_HB 1
+#define LGV_KCLASS_CHARGE 2
+#define LGV_KCLASS_EM 3
+#define LGV_KCLASS_MEASURE 4
+#define LGV_NKCLASS 5
+int lgv_timing_enable(lgv_handle *h, int enable);
+int lgv_timing_read(lgv_handle *h, int kclass, double *total_ms, int64_t *launches);
+
+/* Parity-test aid: when enabled, the next noisy sub-steps record per-decision
+ * flags (0 rejected, 1 accepted with dS < 0, 2 accepted with dS >= 0).
+ * Phi heat bath: flags[n] for site n.  Charge heat bath: flags[(p*6+L-4)*V+nA].
+ * lgv_get_flags copies 36*V bytes. */
+int lgv_debug_flags(lgv_handle *h, int enable);
+int lgv_get_flags(lgv_handle *h, uint8_t *host_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LGV_H */

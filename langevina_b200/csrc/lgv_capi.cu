@@ -1,0 +1,682 @@
+// lgv_capi.cu -- the C ABI of include/lgv.h.
+//
+// The handle owns two red-black SoA lattices (current and alternate, for the
+// stencils that cannot update in place), a staging buffer for the host
+// boundary, and small scratch areas.  It sequences the sub-steps of each
+// reference stepper (Stepper.cxx:542-580) and keeps the 64-bit counter that
+// indexes the noise streams.  No computation happens on the host: a missing
+// or failed kernel surfaces as LGV_ERR_CUDA.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/lgv.h"
+#include "lgv_internal.h"
+
+using lgv::Fields;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+#define LGV_CK(call)                                                                          \
+  do {                                                                                        \
+    cudaError_t e_ = (call);                                                                  \
+    if (e_ != cudaSuccess) return fail(LGV_ERR_CUDA, "%s: %s (%s:%d)", #call,                 \
+                                       cudaGetErrorString(e_), __FILE__, __LINE__);           \
+  } while (0)
+
+#define LGV_TRY(expr)       \
+  do {                      \
+    int r_ = (expr);        \
+    if (r_ != LGV_OK) return r_; \
+  } while (0)
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+// pass orderings of the counter-mode charge step (lexicographic permutations)
+const int kPerm[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
+
+}  // namespace
+
+struct lgv_handle {
+  lgv_params p{};
+  int N = 0;
+  size_t V = 0;
+  int device = 0;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  double *bufA = nullptr, *bufB = nullptr;
+  Fields cur{}, alt{};
+  double *staging = nullptr;
+  double *scratch = nullptr;
+  size_t scratch_len = 0;
+  double *meas_dev = nullptr;
+  double *small_dev = nullptr;  // 8 doubles
+  uint64_t key = 0, ctr = 0;
+  int noise_mode = LGV_NOISE_COUNTER;
+  double *inj_hb_prop = nullptr, *inj_hb_acc = nullptr, *inj_ch_q = nullptr, *inj_ch_acc = nullptr,
+         *inj_em_xi = nullptr;
+  int32_t inj_order[5] = {0, 1, 2, 0, 1};
+  bool have_hb = false, have_ch = false, have_em = false;
+  bool mon_on = false;
+  lgv::MonAcc *mon_dev = nullptr;  // [3]
+  lgv_monitor mon_ideal{};
+  uint8_t *flags_dev = nullptr;
+  // live per-kernel timing (lgv_timing_enable): event pairs around launches
+  bool timing_on = false;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_used;
+  double t_ms[LGV_NKCLASS] = {0};
+  int64_t t_n[LGV_NKCLASS] = {0};
+};
+
+namespace {
+
+int ensure(double **p, size_t n) {
+  if (*p) return LGV_OK;
+  cudaError_t e = cudaMalloc((void **)p, n * sizeof(double));
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return fail(LGV_ERR_NOMEM, "cudaMalloc(%zu doubles): %s", n, cudaGetErrorString(e));
+  }
+  return LGV_OK;
+}
+
+int ensure_scratch(lgv_handle *h, size_t n) {
+  if (h->scratch && h->scratch_len >= n) return LGV_OK;
+  if (h->scratch) cudaFree(h->scratch);
+  h->scratch = nullptr;
+  LGV_TRY(ensure(&h->scratch, n));
+  h->scratch_len = n;
+  return LGV_OK;
+}
+
+int check_params(const lgv_params *p) {
+  if (!p) return fail(LGV_ERR_INVALID, "params is NULL");
+  if (p->N < 4 || (p->N & 1)) return fail(LGV_ERR_INVALID, "N=%d: must be even and >= 4", p->N);
+  if (p->N > 2048) return fail(LGV_ERR_INVALID, "N=%d exceeds the supported 2048", p->N);
+  if (p->reserved0 != 0) return fail(LGV_ERR_INVALID, "reserved0 must be 0");
+  if (!(p->chi > 0)) return fail(LGV_ERR_INVALID, "chi must be > 0");
+  if (!(p->LX > 0)) return fail(LGV_ERR_INVALID, "LX must be > 0");
+  if (!(p->gamma >= 0) || !(p->diffusion >= 0)) return fail(LGV_ERR_INVALID, "gamma, diffusion must be >= 0");
+  return LGV_OK;
+}
+
+Fields fields_of(double *base, size_t V) {
+  Fields f;
+  for (int L = 0; L < 10; ++L) f.c[L] = base + (size_t)L * V;
+  return f;
+}
+
+cudaEvent_t pool_event(lgv_handle *h) {
+  if (!h->ev_pool.empty()) {
+    cudaEvent_t e = h->ev_pool.back();
+    h->ev_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+// Records a CUDA event pair around the launches of one kernel class when
+// timing is enabled; the events are resolved in lgv_timing_read.
+struct KTimer {
+  lgv_handle *h;
+  int cls;
+  cudaEvent_t a = nullptr, b = nullptr;
+  KTimer(lgv_handle *hh, int c) : h(hh), cls(c) {
+    if (!h->timing_on) return;
+    a = pool_event(h);
+    b = pool_event(h);
+    cudaEventRecord(a, h->stream);
+  }
+  ~KTimer() {
+    if (!a) return;
+    cudaEventRecord(b, h->stream);
+    h->ev_used.push_back({cls, {a, b}});
+  }
+};
+
+lgv::MonAcc *mon_ptr(lgv_handle *h, int which) { return h->mon_on ? h->mon_dev + which : nullptr; }
+
+int energy_now(lgv_handle *h, double *E) {
+  LGV_TRY(ensure_scratch(h, lgv::energy_scratch_doubles(h->N)));
+  LGV_TRY(ensure(&h->small_dev, 8));
+  LGV_CK(lgv::launch_energy(h->cur, h->N, h->p.H, 0.5 / h->p.chi, h->scratch, h->small_dev, h->stream));
+  LGV_CK(cudaMemcpyAsync(E, h->small_dev, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  LGV_CK(cudaStreamSynchronize(h->stream));
+  return LGV_OK;
+}
+
+// --- sub-steps -------------------------------------------------------------
+int sub_ideal(lgv_handle *h, double dt) {  // IdealPV2::step (Stepper.cxx:23-66)
+  double Eold = 0, Enew = 0;
+  if (h->mon_on) LGV_TRY(energy_now(h, &Eold));
+  lgv::IdealArgs a;
+  a.dto2chi = (dt / 2.0) / h->p.chi;
+  a.dt = dt;
+  const double hx = h->p.LX / h->N;
+  a.a2 = std::pow(1.0 / hx, 2);
+  a.H = h->p.H;
+  {
+    KTimer tm(h, LGV_KCLASS_IDEAL);
+    LGV_CK(lgv::launch_ideal(h->cur, h->alt, h->N, a, h->stream));
+  }
+  std::swap(h->cur, h->alt);
+  if (h->mon_on) {
+    LGV_TRY(energy_now(h, &Enew));
+    const double dE = Enew - Eold;
+    if (dE > 0) {
+      h->mon_ideal.up_counts++;
+      h->mon_ideal.up_yes++;
+      h->mon_ideal.up_dS += dE;
+    } else {
+      h->mon_ideal.down_counts++;
+      h->mon_ideal.down_dS += dE;
+    }
+  }
+  return LGV_OK;
+}
+
+int sub_hb(lgv_handle *h, double dt, double mass) {  // EulerLangevinHB::step (Stepper.cxx:287-389)
+  lgv::HbArgs a{};
+  a.rdtg = std::sqrt(2. * dt * h->p.gamma);
+  a.Lambda2 = 0.5 * (2. * 3. + mass);
+  a.lam4 = h->p.lambda / 4.;
+  a.H = h->p.H;
+  a.mon = mon_ptr(h, LGV_MONITOR_PHI_HB);
+  a.flags = h->flags_dev;
+  if (h->noise_mode == LGV_NOISE_INJECTED) {
+    if (!h->have_hb) return fail(LGV_ERR_STATE, "phi heat bath: injected noise not supplied");
+    a.prop = h->inj_hb_prop;
+    a.acc = h->inj_hb_acc;
+  } else {
+    a.sk = lgv::sub_key(h->key, h->ctr);
+  }
+  for (int parity = 0; parity < 2; ++parity) {
+    KTimer tm(h, LGV_KCLASS_PHI_HB);
+    LGV_CK(lgv::launch_hb_pass(h->cur, h->N, parity, a, h->stream));
+  }
+  if (h->noise_mode == LGV_NOISE_INJECTED) h->have_hb = false;
+  else h->ctr += 1;
+  return LGV_OK;
+}
+
+int sub_charge(lgv_handle *h, double dt) {  // ModelGChargeHB::step (Stepper.cxx:449-522)
+  int xyz[3] = {0, 1, 2}, eo[2] = {0, 1};
+  if (h->noise_mode == LGV_NOISE_INJECTED) {
+    if (!h->have_ch) return fail(LGV_ERR_STATE, "charge heat bath: injected noise not supplied");
+    for (int a = 0; a < 3; ++a) xyz[a] = h->inj_order[a];
+    eo[0] = h->inj_order[3];
+    eo[1] = h->inj_order[4];
+  } else {
+    const uint64_t w = lgv::split_word(lgv::sub_key(h->key, h->ctr), 0);
+    const int pi = (int)((w & 0xffffffffull) % 6ull);
+    for (int a = 0; a < 3; ++a) xyz[a] = kPerm[pi][a];
+    if (w >> 63) {
+      eo[0] = 1;
+      eo[1] = 0;
+    }
+  }
+  lgv::ChargeArgs a{};
+  a.rms = std::sqrt(2. * dt * (h->p.diffusion * h->p.chi));
+  a.inv2chi = 1.0 / (2. * h->p.chi);
+  a.mon = mon_ptr(h, LGV_MONITOR_CHARGE_HB);
+  a.flags = h->flags_dev;
+  if (h->noise_mode == LGV_NOISE_INJECTED) {
+    a.q = h->inj_ch_q;
+    a.acc = h->inj_ch_acc;
+  }
+  for (int p = 0; p < 6; ++p) {
+    a.pass = p;
+    if (h->noise_mode != LGV_NOISE_INJECTED) a.sk = lgv::sub_key(h->key, h->ctr + 1 + p);
+    KTimer tm(h, LGV_KCLASS_CHARGE);
+    LGV_CK(lgv::launch_charge_pass(h->cur, h->N, xyz[p / 2], eo[p % 2], a, h->stream));
+  }
+  if (h->noise_mode == LGV_NOISE_INJECTED) h->have_ch = false;
+  else h->ctr += 7;
+  return LGV_OK;
+}
+
+int sub_em(lgv_handle *h, double dt, double mass) {
+  lgv::EmArgs a{};
+  a.c6 = 6.0 + mass;
+  a.dtg = dt * h->p.gamma;
+  a.sq = std::sqrt(2.0 * h->p.gamma * dt);
+  a.lambda = h->p.lambda;
+  a.H = h->p.H;
+  if (h->noise_mode == LGV_NOISE_INJECTED) {
+    if (!h->have_em) return fail(LGV_ERR_STATE, "Euler-Maruyama: injected noise not supplied");
+    a.xi = h->inj_em_xi;
+  } else {
+    a.sk = lgv::sub_key(h->key, h->ctr);
+  }
+  {
+    KTimer tm(h, LGV_KCLASS_EM);
+    LGV_CK(lgv::launch_em(h->cur, h->alt, h->N, a, h->stream));
+  }
+  for (int l = 0; l < 4; ++l) std::swap(h->cur.c[l], h->alt.c[l]);
+  if (h->noise_mode == LGV_NOISE_INJECTED) h->have_em = false;
+  else h->ctr += 1;
+  return LGV_OK;
+}
+
+int step_once(lgv_handle *h, int ev, int inner, int outer, double dt, double t) {
+  const double mass = h->p.mass0 + h->p.dmassdt * t;  // ModelACoefficients::mass (ModelA.h:84)
+  switch (ev) {
+    case LGV_PV2HBSPLIT:
+    case LGV_PV2HBSPLIT_NODIFFUSE:
+    case LGV_PV2HBSPLIT_ONLYDIFFUSE:
+      if (ev != LGV_PV2HBSPLIT_ONLYDIFFUSE) {
+        for (int i1 = 0; i1 < outer; ++i1) {
+          LGV_TRY(sub_ideal(h, dt / (unsigned)outer));
+          for (int i0 = 0; i0 < inner; ++i0) LGV_TRY(sub_hb(h, dt / ((unsigned)inner * (unsigned)outer), mass));
+        }
+      }
+      if (ev != LGV_PV2HBSPLIT_NODIFFUSE) LGV_TRY(sub_charge(h, dt));
+      return LGV_OK;
+    case LGV_IDEAL_PV2: return sub_ideal(h, dt);
+    case LGV_EULER_LANGEVIN_HB: return sub_hb(h, dt, mass);
+    case LGV_CHARGE_HB: return sub_charge(h, dt);
+    case LGV_MODELA_EM: return sub_em(h, dt, mass);
+    default: return fail(LGV_ERR_INVALID, "unknown evolver %d", ev);
+  }
+}
+
+int copy_injected(double **dst, const double *src, size_t n) {
+  LGV_TRY(ensure(dst, n));
+  LGV_CK(cudaMemcpy(*dst, src, n * sizeof(double), cudaMemcpyHostToDevice));
+  return LGV_OK;
+}
+
+}  // namespace
+
+// ============================================================================
+extern "C" {
+
+int lgv_version(void) { return 10000; }
+
+const char *lgv_status_string(int s) {
+  switch (s) {
+    case LGV_OK: return "ok";
+    case LGV_ERR_INVALID: return "invalid argument";
+    case LGV_ERR_CUDA: return "CUDA error";
+    case LGV_ERR_NOMEM: return "out of memory";
+    case LGV_ERR_TIMEOUT: return "device wait timed out";
+    case LGV_ERR_STATE: return "invalid state";
+    case LGV_ERR_UNSUPPORTED: return "unsupported";
+    default: return "unknown status";
+  }
+}
+
+const char *lgv_last_error(void) { return g_last_error.c_str(); }
+
+int lgv_create(const lgv_params *params, lgv_handle **out) {
+  if (!out) return fail(LGV_ERR_INVALID, "out is NULL");
+  *out = nullptr;
+  LGV_TRY(check_params(params));
+  int dev = 0;
+  LGV_CK(cudaGetDevice(&dev));
+  lgv_handle *h = new lgv_handle();
+  h->p = *params;
+  h->N = params->N;
+  h->V = (size_t)h->N * h->N * h->N;
+  h->device = dev;
+  h->key = lgv::make_key(params->seed);
+  int rc = LGV_OK;
+  if (cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    rc = fail(LGV_ERR_CUDA, "cudaStreamCreate failed");
+  }
+  h->stream = h->own_stream;
+  if (rc == LGV_OK) rc = ensure(&h->bufA, 10 * h->V);
+  if (rc == LGV_OK) rc = ensure(&h->bufB, 10 * h->V);
+  if (rc == LGV_OK) rc = ensure(&h->small_dev, 8);
+  if (rc == LGV_OK) {
+    cudaError_t e = cudaMalloc((void **)&h->mon_dev, 3 * sizeof(lgv::MonAcc));
+    if (e != cudaSuccess) rc = fail(LGV_ERR_NOMEM, "monitor alloc: %s", cudaGetErrorString(e));
+  }
+  if (rc == LGV_OK) {
+    h->cur = fields_of(h->bufA, h->V);
+    h->alt = fields_of(h->bufB, h->V);
+    if (cudaMemsetAsync(h->bufA, 0, 10 * h->V * sizeof(double), h->stream) != cudaSuccess ||
+        cudaMemsetAsync(h->mon_dev, 0, 3 * sizeof(lgv::MonAcc), h->stream) != cudaSuccess ||
+        cudaStreamSynchronize(h->stream) != cudaSuccess)
+      rc = fail(LGV_ERR_CUDA, "initial memset failed");
+  }
+  if (rc != LGV_OK) {
+    lgv_destroy(h);
+    return rc;
+  }
+  *out = h;
+  return LGV_OK;
+}
+
+int lgv_destroy(lgv_handle *h) {
+  if (!h) return LGV_OK;
+  DeviceGuard g(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  double *bufs[] = {h->bufA, h->bufB, h->staging, h->scratch, h->meas_dev, h->small_dev, h->inj_hb_prop,
+                    h->inj_hb_acc, h->inj_ch_q, h->inj_ch_acc, h->inj_em_xi};
+  for (double *b : bufs)
+    if (b) cudaFree(b);
+  if (h->mon_dev) cudaFree(h->mon_dev);
+  if (h->flags_dev) cudaFree(h->flags_dev);
+  for (auto &u : h->ev_used) {
+    cudaEventDestroy(u.second.first);
+    cudaEventDestroy(u.second.second);
+  }
+  for (auto e : h->ev_pool) cudaEventDestroy(e);
+  if (h->own_stream) cudaStreamDestroy(h->own_stream);
+  delete h;
+  return LGV_OK;
+}
+
+int lgv_set_params(lgv_handle *h, const lgv_params *params) {
+  if (!h) return fail(LGV_ERR_INVALID, "handle is NULL");
+  LGV_TRY(check_params(params));
+  if (params->N != h->N) return fail(LGV_ERR_INVALID, "N cannot change (%d -> %d)", h->N, params->N);
+  if (params->seed != h->p.seed) h->key = lgv::make_key(params->seed);
+  h->p = *params;
+  return LGV_OK;
+}
+
+int lgv_set_state(lgv_handle *h, const double *host_aos) {
+  if (!h || !host_aos) return fail(LGV_ERR_INVALID, "NULL argument");
+  DeviceGuard g(h->device);
+  LGV_TRY(ensure(&h->staging, 10 * h->V));
+  LGV_CK(cudaMemcpyAsync(h->staging, host_aos, 10 * h->V * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  LGV_CK(lgv::launch_aos_to_rb(h->staging, h->cur, h->N, h->stream));
+  LGV_CK(cudaStreamSynchronize(h->stream));
+  return LGV_OK;
+}
+
+int lgv_get_state(lgv_handle *h, double *host_aos) {
+  if (!h || !host_aos) return fail(LGV_ERR_INVALID, "NULL argument");
+  DeviceGuard g(h->device);
+  LGV_TRY(ensure(&h->staging, 10 * h->V));
+  LGV_CK(lgv::launch_rb_to_aos(h->cur, h->staging, h->N, h->stream));
+  LGV_CK(cudaMemcpyAsync(host_aos, h->staging, 10 * h->V * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  LGV_CK(cudaStreamSynchronize(h->stream));
+  return LGV_OK;
+}
+
+int lgv_set_state_device(lgv_handle *h, const double *dev_aos) {
+  if (!h || !dev_aos) return fail(LGV_ERR_INVALID, "NULL argument");
+  DeviceGuard g(h->device);
+  LGV_CK(lgv::launch_aos_to_rb(dev_aos, h->cur, h->N, h->stream));
+  return LGV_OK;
+}
+
+int lgv_get_state_device(lgv_handle *h, double *dev_aos) {
+  if (!h || !dev_aos) return fail(LGV_ERR_INVALID, "NULL argument");
+  DeviceGuard g(h->device);
+  LGV_CK(lgv::launch_rb_to_aos(h->cur, dev_aos, h->N, h->stream));
+  return LGV_OK;
+}
+
+int lgv_initialize(lgv_handle *h, int kind, double scale) {
+  if (!h) return fail(LGV_ERR_INVALID, "handle is NULL");
+  DeviceGuard g(h->device);
+  switch (kind) {
+    case LGV_INIT_ZERO:
+      for (int L = 0; L < 10; ++L) LGV_CK(cudaMemsetAsync(h->cur.c[L], 0, h->V * sizeof(double), h->stream));
+      return LGV_OK;
+    case LGV_INIT_PHI_GAUSSIAN:
+      LGV_CK(lgv::launch_init_phi(h->cur, h->N, lgv::sub_key(h->key, h->ctr), scale, h->stream));
+      h->ctr += 1;
+      return LGV_OK;
+    case LGV_INIT_CHARGES_GAUSSIAN: {
+      const size_t nb = (h->V + 255) / 256;
+      LGV_TRY(ensure_scratch(h, nb * 6 + 16));
+      LGV_CK(lgv::launch_init_charges(h->cur, h->N, lgv::sub_key(h->key, h->ctr), std::sqrt(h->p.chi), h->scratch,
+                                      h->stream));
+      h->ctr += 1;
+      return LGV_OK;
+    }
+    default: return fail(LGV_ERR_INVALID, "unknown init kind %d", kind);
+  }
+}
+
+int lgv_set_noise_mode(lgv_handle *h, int mode) {
+  if (!h) return fail(LGV_ERR_INVALID, "handle is NULL");
+  if (mode != LGV_NOISE_COUNTER && mode != LGV_NOISE_INJECTED) return fail(LGV_ERR_INVALID, "noise mode %d", mode);
+  h->noise_mode = mode;
+  return LGV_OK;
+}
+
+int lgv_set_counter(lgv_handle *h, uint64_t c) {
+  if (!h) return fail(LGV_ERR_INVALID, "handle is NULL");
+  h->ctr = c;
+  return LGV_OK;
+}
+
+int lgv_get_counter(lgv_handle *h, uint64_t *c) {
+  if (!h || !c) return fail(LGV_ERR_INVALID, "NULL argument");
+  *c = h->ctr;
+  return LGV_OK;
+}
+
+int lgv_inject_hb(lgv_handle *h, const double *prop, const double *acc) {
+  if (!h || !prop || !acc) return fail(LGV_ERR_INVALID, "NULL argument");
+  DeviceGuard g(h->device);
+  LGV_TRY(copy_injected(&h->inj_hb_prop, prop, 4 * h->V));
+  LGV_TRY(copy_injected(&h->inj_hb_acc, acc, h->V));
+  h->have_hb = true;
+  return LGV_OK;
+}
+
+int lgv_inject_charge(lgv_handle *h, const int32_t *order, const double *q, const double *acc) {
+  if (!h || !order || !q || !acc) return fail(LGV_ERR_INVALID, "NULL argument");
+  bool seen[3] = {false, false, false};
+  for (int a = 0; a < 3; ++a) {
+    if (order[a] < 0 || order[a] > 2 || seen[order[a]]) return fail(LGV_ERR_INVALID, "order[0:3] not a permutation");
+    seen[order[a]] = true;
+  }
+  if (!((order[3] == 0 && order[4] == 1) || (order[3] == 1 && order[4] == 0)))
+    return fail(LGV_ERR_INVALID, "order[3:5] not a permutation of (0,1)");
+  DeviceGuard g(h->device);
+  LGV_TRY(copy_injected(&h->inj_ch_q, q, 36 * h->V));
+  LGV_TRY(copy_injected(&h->inj_ch_acc, acc, 36 * h->V));
+  for (int a = 0; a < 5; ++a) h->inj_order[a] = order[a];
+  h->have_ch = true;
+  return LGV_OK;
+}
+
+int lgv_inject_em(lgv_handle *h, const double *xi) {
+  if (!h || !xi) return fail(LGV_ERR_INVALID, "NULL argument");
+  DeviceGuard g(h->device);
+  LGV_TRY(copy_injected(&h->inj_em_xi, xi, 4 * h->V));
+  h->have_em = true;
+  return LGV_OK;
+}
+
+int lgv_step(lgv_handle *h, int evolver, int inner, int outer, double dt, double t, int nsteps) {
+  if (!h) return fail(LGV_ERR_INVALID, "handle is NULL");
+  if (nsteps < 0) return fail(LGV_ERR_INVALID, "nsteps < 0");
+  if (evolver <= LGV_PV2HBSPLIT_ONLYDIFFUSE && (inner < 1 || outer < 1))
+    return fail(LGV_ERR_INVALID, "PV2HBSplit scounts must be >= 1 (got {%d, %d})", inner, outer);
+  if (!std::isfinite(dt) || !std::isfinite(t)) return fail(LGV_ERR_INVALID, "dt/t not finite");
+  DeviceGuard g(h->device);
+  for (int s = 0; s < nsteps; ++s) {
+    LGV_TRY(step_once(h, evolver, inner, outer, dt, t));
+    t += dt;
+  }
+  return LGV_OK;
+}
+
+size_t lgv_measure_size(int N) { return lgv::measure_size(N); }
+
+int lgv_measure_device(lgv_handle *h, double *dev_out) {
+  if (!h || !dev_out) return fail(LGV_ERR_INVALID, "NULL argument");
+  DeviceGuard g(h->device);
+  LGV_TRY(ensure_scratch(h, lgv::measure_scratch_doubles(h->N)));
+  KTimer tm(h, LGV_KCLASS_MEASURE);
+  LGV_CK(lgv::launch_measure(h->cur, h->N, h->scratch, dev_out, h->stream));
+  return LGV_OK;
+}
+
+int lgv_measure(lgv_handle *h, lgv_measurement *out) {
+  if (!h || !out) return fail(LGV_ERR_INVALID, "NULL argument");
+  DeviceGuard g(h->device);
+  const size_t n = lgv::measure_size(h->N);
+  LGV_TRY(ensure(&h->meas_dev, n));
+  LGV_TRY(lgv_measure_device(h, h->meas_dev));
+  std::vector<double> host(n);
+  LGV_CK(cudaMemcpyAsync(host.data(), h->meas_dev, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  LGV_CK(cudaStreamSynchronize(h->stream));
+  const int N = h->N, NK = N / 2 + 1;
+  const double *p = host.data();
+  auto take = [&](double *dst, size_t cnt) {
+    if (dst) std::memcpy(dst, p, cnt * sizeof(double));
+    p += cnt;
+  };
+  take(out->OAverage, 11);
+  for (int a = 0; a < 3; ++a) take(out->wall[a], 11 * (size_t)N);
+  for (int a = 0; a < 3; ++a) take(out->wall_k[a], 11 * (size_t)NK * 2);
+  for (int a = 0; a < 3; ++a) take(out->wall_k_rotated[a], 14 * (size_t)NK * 2);
+  for (int a = 0; a < 3; ++a) take(out->wall_phase[a], 14 * (size_t)N);
+  for (int a = 0; a < 3; ++a) take(out->wall_phase_k[a], 14 * (size_t)NK * 2);
+  return LGV_OK;
+}
+
+int lgv_energy(lgv_handle *h, double *energy) {
+  if (!h || !energy) return fail(LGV_ERR_INVALID, "NULL argument");
+  DeviceGuard g(h->device);
+  return energy_now(h, energy);
+}
+
+int lgv_enable_monitors(lgv_handle *h, int enable) {
+  if (!h) return fail(LGV_ERR_INVALID, "handle is NULL");
+  DeviceGuard g(h->device);
+  h->mon_on = enable != 0;
+  h->mon_ideal = lgv_monitor{};
+  LGV_CK(cudaMemsetAsync(h->mon_dev, 0, 3 * sizeof(lgv::MonAcc), h->stream));
+  LGV_CK(cudaStreamSynchronize(h->stream));
+  return LGV_OK;
+}
+
+int lgv_get_monitor(lgv_handle *h, int which, lgv_monitor *out) {
+  if (!h || !out) return fail(LGV_ERR_INVALID, "NULL argument");
+  if (which < 0 || which > 2) return fail(LGV_ERR_INVALID, "monitor %d", which);
+  if (which == LGV_MONITOR_IDEAL) {
+    *out = h->mon_ideal;
+    return LGV_OK;
+  }
+  DeviceGuard g(h->device);
+  lgv::MonAcc m;
+  LGV_CK(cudaMemcpyAsync(&m, h->mon_dev + which, sizeof(m), cudaMemcpyDeviceToHost, h->stream));
+  LGV_CK(cudaStreamSynchronize(h->stream));
+  out->down_counts = (int64_t)m.down_counts;
+  out->up_counts = (int64_t)m.up_counts;
+  out->up_yes = (int64_t)m.up_yes;
+  out->up_no = (int64_t)m.up_no;
+  out->down_dS = m.down_dS;
+  out->up_dS = m.up_dS;
+  return LGV_OK;
+}
+
+int lgv_set_stream(lgv_handle *h, void *s) {
+  if (!h) return fail(LGV_ERR_INVALID, "handle is NULL");
+  h->stream = s ? (cudaStream_t)s : h->own_stream;
+  return LGV_OK;
+}
+
+int lgv_synchronize(lgv_handle *h) {
+  if (!h) return fail(LGV_ERR_INVALID, "handle is NULL");
+  DeviceGuard g(h->device);
+  LGV_CK(cudaStreamSynchronize(h->stream));
+  return LGV_OK;
+}
+
+int lgv_timing_enable(lgv_handle *h, int enable) {
+  if (!h) return fail(LGV_ERR_INVALID, "handle is NULL");
+  DeviceGuard g(h->device);
+  LGV_CK(cudaStreamSynchronize(h->stream));
+  for (auto &u : h->ev_used) {
+    h->ev_pool.push_back(u.second.first);
+    h->ev_pool.push_back(u.second.second);
+  }
+  h->ev_used.clear();
+  for (int c = 0; c < LGV_NKCLASS; ++c) {
+    h->t_ms[c] = 0;
+    h->t_n[c] = 0;
+  }
+  h->timing_on = enable != 0;
+  return LGV_OK;
+}
+
+int lgv_timing_read(lgv_handle *h, int kclass, double *total_ms, int64_t *launches) {
+  if (!h || !total_ms || !launches) return fail(LGV_ERR_INVALID, "NULL argument");
+  if (kclass < 0 || kclass >= LGV_NKCLASS) return fail(LGV_ERR_INVALID, "kernel class %d", kclass);
+  DeviceGuard g(h->device);
+  LGV_CK(cudaStreamSynchronize(h->stream));
+  for (auto &u : h->ev_used) {
+    float ms = 0;
+    LGV_CK(cudaEventElapsedTime(&ms, u.second.first, u.second.second));
+    h->t_ms[u.first] += ms;
+    h->t_n[u.first] += 1;
+    h->ev_pool.push_back(u.second.first);
+    h->ev_pool.push_back(u.second.second);
+  }
+  h->ev_used.clear();
+  *total_ms = h->t_ms[kclass];
+  *launches = h->t_n[kclass];
+  return LGV_OK;
+}
+
+int lgv_debug_flags(lgv_handle *h, int enable) {
+  if (!h) return fail(LGV_ERR_INVALID, "handle is NULL");
+  DeviceGuard g(h->device);
+  if (enable) {
+    if (!h->flags_dev) {
+      cudaError_t e = cudaMalloc((void **)&h->flags_dev, 36 * h->V);
+      if (e != cudaSuccess) return fail(LGV_ERR_NOMEM, "flags alloc: %s", cudaGetErrorString(e));
+    }
+    LGV_CK(cudaMemsetAsync(h->flags_dev, 0, 36 * h->V, h->stream));
+  } else if (h->flags_dev) {
+    LGV_CK(cudaStreamSynchronize(h->stream));
+    cudaFree(h->flags_dev);
+    h->flags_dev = nullptr;
+  }
+  return LGV_OK;
+}
+
+int lgv_get_flags(lgv_handle *h, uint8_t *host_out) {
+  if (!h || !host_out) return fail(LGV_ERR_INVALID, "NULL argument");
+  if (!h->flags_dev) return fail(LGV_ERR_STATE, "debug flags not enabled");
+  DeviceGuard g(h->device);
+  LGV_CK(cudaMemcpyAsync(host_out, h->flags_dev, 36 * h->V, cudaMemcpyDeviceToHost, h->stream));
+  LGV_CK(cudaStreamSynchronize(h->stream));
+  return LGV_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,177 @@
+// lgv_device.cuh -- device-side building blocks of the B200 stepper.
+//
+// Lattice layout in HBM ("red-black SoA"):
+//   Fields holds one pointer per site component L = 0..9 (phi_0..3, A_1..3,
+//   V_1..3, the order of data_node::x, ModelA.h:283-286).  Each component
+//   plane holds V = N^3 doubles split by checkerboard parity p = (i+j+k)&1:
+//     plane[p * V/2 + (k*N + j) * N/2 + (i >> 1)].
+//   In a row (j, k) the sites of parity p sit at i = 2m + ((p + j + k) & 1).
+//   A parity pass of the heat baths therefore reads and writes whole
+//   contiguous half-rows: every load and store is coalesced and nothing of
+//   the other parity is rewritten.
+#pragma once
+
+#include <cstdint>
+
+namespace lgv {
+
+struct Fields {
+  double *c[10];
+};
+
+// Geometry helpers -----------------------------------------------------------
+struct Geo {
+  int N;      // lattice extent
+  int H;      // N / 2
+  long long V2;  // V / 2
+};
+
+__host__ __device__ __forceinline__ Geo make_geo(int N) {
+  Geo g;
+  g.N = N;
+  g.H = N >> 1;
+  g.V2 = (long long)N * N * (N >> 1);
+  return g;
+}
+
+// red-black offset of natural site (i, j, k) inside a component plane
+__host__ __device__ __forceinline__ long long rb_off(const Geo &g, int i, int j, int k) {
+  return (long long)((i + j + k) & 1) * g.V2 + ((long long)k * g.N + j) * g.H + (i >> 1);
+}
+
+__device__ __forceinline__ int wrap_inc(int a, int n) { return (a + 1 == n) ? 0 : a + 1; }
+__device__ __forceinline__ int wrap_dec(int a, int n) { return (a == 0) ? n - 1 : a - 1; }
+
+// Counter-indexed xoroshiro128+ streams -------------------------------------
+// A stream is identified by (sub-step key sk, index n); its 128-bit state is
+// splitmix64 outputs 2n and 2n+1 of the sequence seeded with sk.  The engine
+// is the reference's xoroshiro128+ (rotations 55/14/36,
+// xoroshiro128plus.h:261-271).
+static constexpr uint64_t kGolden = 0x9E3779B97F4A7C15ull;
+
+__host__ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+__host__ __device__ __forceinline__ uint64_t make_key(uint64_t seed) { return mix64(seed + kGolden); }
+__host__ __device__ __forceinline__ uint64_t sub_key(uint64_t key, uint64_t ctr) {
+  return mix64(key + (ctr + 1) * kGolden);
+}
+__host__ __device__ __forceinline__ uint64_t split_word(uint64_t sk, uint64_t w) {
+  return mix64(sk + (w + 1) * kGolden);
+}
+
+struct Xoro {
+  uint64_t s0, s1;
+  __device__ __forceinline__ uint64_t next() {
+    const uint64_t a = s0;
+    uint64_t b = s1;
+    const uint64_t r = a + b;
+    b ^= a;
+    s0 = ((a << 55) | (a >> 9)) ^ b ^ (b << 14);
+    s1 = (b << 36) | (b >> 28);
+    return r;
+  }
+};
+
+__device__ __forceinline__ Xoro stream_at(uint64_t sk, uint64_t n) {
+  Xoro x;
+  x.s0 = split_word(sk, 2 * n);
+  x.s1 = split_word(sk, 2 * n + 1);
+  return x;
+}
+
+// uniform in [0,1) from the top 53 bits (exact conversion)
+__device__ __forceinline__ double u53(uint64_t r) { return (double)(r >> 11) * 0x1p-53; }
+// variance-1 uniform in [-sqrt3, sqrt3): (2u - 1) is exact, one rounding in the product
+__device__ __forceinline__ double var1(uint64_t r) {
+  const double t = 2.0 * u53(r) - 1.0;
+  return __dmul_rn(t, 1.7320508075688772);
+}
+// Box-Muller pair, u1 = 1 - u53(ra) in (0,1], angle 2*pi*u53(rb)
+__device__ __forceinline__ void box_muller(uint64_t ra, uint64_t rb, double &z0, double &z1) {
+  const double u1 = 1.0 - u53(ra);
+  const double u2 = u53(rb);
+  const double rho = sqrt(-2.0 * log(u1));
+  double s, c;
+  sincospi(2.0 * u2, &s, &c);
+  z0 = rho * c;
+  z1 = rho * s;
+}
+
+// O(4) algebra (O4AlgebraHelper.h:17-97) ------------------------------------
+// expmul(v) = (cos|v|, -sin|v|/|v| * v).  For |v|^2 <= 1/16 the cosine and
+// sin(x)/x come from their Maclaurin series in x^2 (terms through x^12 keep
+// the truncation below 1e-17 relative); larger angles use sincos().  Below
+// |v| = 1e-20 the identity is returned, as in the reference.
+__device__ __forceinline__ void cos_sinc(double x2, double &c, double &sc) {
+  if (x2 <= 0.0625) {
+    // cos x = sum (-1)^n x^2n/(2n)!,  sin x / x = sum (-1)^n x^2n/(2n+1)!
+    c = 1.0 / 479001600.0;                 // 1/12!
+    c = fma(c, -x2, 1.0 / 3628800.0);      // 1/10!
+    c = fma(c, -x2, 1.0 / 40320.0);        // 1/8!
+    c = fma(c, -x2, 1.0 / 720.0);          // 1/6!
+    c = fma(c, -x2, 1.0 / 24.0);           // 1/4!
+    c = fma(c, -x2, 1.0 / 2.0);            // 1/2!
+    c = fma(c, -x2, 1.0);
+    sc = 1.0 / 6227020800.0;               // 1/13!
+    sc = fma(sc, -x2, 1.0 / 39916800.0);   // 1/11!
+    sc = fma(sc, -x2, 1.0 / 362880.0);     // 1/9!
+    sc = fma(sc, -x2, 1.0 / 5040.0);       // 1/7!
+    sc = fma(sc, -x2, 1.0 / 120.0);        // 1/5!
+    sc = fma(sc, -x2, 1.0 / 6.0);          // 1/3!
+    sc = fma(sc, -x2, 1.0);
+  } else {
+    const double a = sqrt(x2);
+    double s;
+    sincos(a, &s, &c);
+    sc = s / a;
+  }
+}
+
+__device__ __forceinline__ void expmul(const double v0, const double v1, const double v2, double w[4]) {
+  const double x2 = v0 * v0 + v1 * v1 + v2 * v2;
+  if (x2 > 1e-40) {
+    double c, sc;
+    cos_sinc(x2, c, sc);
+    w[0] = c;
+    w[1] = -sc * v0;
+    w[2] = -sc * v1;
+    w[3] = -sc * v2;
+  } else {
+    w[0] = 1.0;
+    w[1] = w[2] = w[3] = 0.0;
+  }
+}
+
+// w = v1 * v2 as quaternions (scalar, vector): (a0 b0 - a.b, a x b + b0 a + a0 b)
+__device__ __forceinline__ void quatmul(const double a[4], const double b[4], double w[4]) {
+  w[0] = a[0] * b[0] - (a[1] * b[1] + a[2] * b[2] + a[3] * b[3]);
+  w[1] = (a[2] * b[3] - b[2] * a[3]) + b[0] * a[1] + a[0] * b[1];
+  w[2] = (a[3] * b[1] - a[1] * b[3]) + b[0] * a[2] + a[0] * b[2];
+  w[3] = (a[1] * b[2] - b[1] * a[2]) + b[0] * a[3] + a[0] * b[3];
+}
+
+// In-place O(4) rotation phi <- L phi R with R = exp(-(muV - muA)/2),
+// L = exp((muV + muA)/2) (O4Rotation, O4AlgebraHelper.h:78-97).
+__device__ __forceinline__ void o4_rotate(const double muV[3], const double muA[3], double phi[4]) {
+  double R[4], L[4], t[4];
+  expmul(-0.5 * (muV[0] - muA[0]), -0.5 * (muV[1] - muA[1]), -0.5 * (muV[2] - muA[2]), R);
+  expmul(0.5 * (muV[0] + muA[0]), 0.5 * (muV[1] + muA[1]), 0.5 * (muV[2] + muA[2]), L);
+  quatmul(phi, R, t);
+  quatmul(L, t, phi);
+}
+
+// rotatePhi for one site (Stepper.cxx:178-202): mu = -n / chi * dt
+__device__ __forceinline__ void rotate_site(double phi[4], const double q[6], double dt_over_chi) {
+  double muA[3], muV[3];
+#pragma unroll
+  for (int s = 0; s < 3; ++s) {
+    muA[s] = -q[s] * dt_over_chi;
+    muV[s] = -q[3 + s] * dt_over_chi;
+  }
+  o4_rotate(muV, muA, phi);
+}
+
+}  // namespace lgv

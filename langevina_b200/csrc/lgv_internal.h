@@ -1,0 +1,79 @@
+// lgv_internal.h -- host-side declarations shared by the kernel and C-ABI
+// translation units of liblgv.so (not installed, not part of the ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "lgv_device.cuh"
+
+namespace lgv {
+
+// Device monitor accumulator (o4_stepper_monitor, Stepper.h:17-49).
+struct MonAcc {
+  unsigned long long down_counts, up_counts, up_yes, up_no;
+  double down_dS, up_dS;
+};
+
+struct HbArgs {
+  double rdtg;     // sqrt(2 dt gamma)
+  double Lambda2;  // (6 + m^2) / 2
+  double lam4;     // lambda / 4
+  double H;
+  uint64_t sk;          // sub-step key (counter mode)
+  const double *prop;   // injected [4][V] or null
+  const double *acc;    // injected [V] or null
+  uint8_t *flags;       // [V] or null
+  MonAcc *mon;          // or null
+};
+
+struct ChargeArgs {
+  double rms;       // sqrt(2 dt sigma)
+  double inv2chi;   // 1 / (2 chi)
+  uint64_t sk;
+  int pass;         // position 0..5 in the step (injected indexing / flags)
+  const double *q;    // injected [6][6][V] or null
+  const double *acc;  // injected [6][6][V] or null
+  uint8_t *flags;     // [36 V] or null
+  MonAcc *mon;
+};
+
+struct EmArgs {
+  double c6;    // 6 + m^2
+  double dtg;   // dt * gamma
+  double sq;    // sqrt(2 gamma dt)
+  double lambda;
+  double H;
+  uint64_t sk;
+  const double *xi;  // injected [4][V] or null
+};
+
+struct IdealArgs {
+  double dto2chi;  // (dt / 2) / chi  : half-step rotation angle per unit charge
+  double dt;
+  double a2;       // (1 / h)^2
+  double H;
+};
+
+// Launchers (lgv_kernels.cu).  All asynchronous on `st`; return cudaError_t.
+cudaError_t launch_aos_to_rb(const double *aos, Fields f, int N, cudaStream_t st);
+cudaError_t launch_rb_to_aos(Fields f, double *aos, int N, cudaStream_t st);
+cudaError_t launch_init_phi(Fields f, int N, uint64_t sk, double scale, cudaStream_t st);
+cudaError_t launch_init_charges(Fields f, int N, uint64_t sk, double sqrtchi, double *scratch,
+                                cudaStream_t st);
+cudaError_t launch_hb_pass(Fields f, int N, int parity, const HbArgs &a, cudaStream_t st);
+cudaError_t launch_charge_pass(Fields f, int N, int dir, int eoA, const ChargeArgs &a, cudaStream_t st);
+cudaError_t launch_em(Fields in, Fields out, int N, const EmArgs &a, cudaStream_t st);
+cudaError_t launch_ideal(Fields in, Fields out, int N, const IdealArgs &a, cudaStream_t st);
+// energy: writes E into dev_out[0]; scratch >= energy_scratch_doubles(N)
+size_t energy_scratch_doubles(int N);
+cudaError_t launch_energy(Fields f, int N, double H, double inv2chi_half, double *scratch, double *dev_out,
+                          cudaStream_t st);
+// measurement: dev_out receives measure_size(N) doubles (lgv.h packing);
+// scratch >= measure_scratch_doubles(N)
+size_t measure_size(int N);
+size_t measure_scratch_doubles(int N);
+cudaError_t launch_measure(Fields f, int N, double *scratch, double *dev_out, cudaStream_t st);
+
+}  // namespace lgv
