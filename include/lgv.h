@@ -216,6 +216,25 @@ int lgv_timing_read(lgv_handle *h, int kclass, double *total_ms, int64_t *launch
 int lgv_debug_flags(lgv_handle *h, int enable);
 int lgv_get_flags(lgv_handle *h, uint8_t *host_out);
 
+/* Allocation-free measurement.  No counterpart in the reference: it is the
+ * measurement of lgv_measure_device() for callers that cannot allocate device
+ * memory while they run -- a host whose GPU memory belongs to another
+ * allocator (a framework's caching pool that has reserved most of the device,
+ * where an extra cudaMalloc can fail even though the pool has room) or a
+ * process held to a fixed device-memory budget.  The caller passes the lattice
+ * (dev_aos: N^3 * 10 doubles in device memory, the host-order AoS layout of
+ * lgv_set_state) and the output (dev_out: lgv_measure_size(N) doubles in device
+ * memory, packed as for lgv_measure_device) and needs no handle.  Scratch space
+ * is a static device array inside the library sized for N <= 128 (6.55 MB,
+ * held on every GPU that loads the library until exit); larger N is rejected
+ * with LGV_ERR_INVALID.  The array is shared by all calls on a device, so calls
+ * whose kernels overlap on the GPU race with each other.  The first call on a
+ * device looks the array up (cudaGetSymbolAddress) with that device current;
+ * make that first call before any stream capture.  Asynchronous on `stream`
+ * (NULL = legacy default stream); calls no allocator. */
+#define LGV_NOALLOC_MAX_N 128
+int lgv_measure_aos_noalloc(const double *dev_aos, int N, double *dev_out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

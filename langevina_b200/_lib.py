@@ -14,6 +14,7 @@ LIB_PATH = os.path.join(HERE, "liblgv.so")
 LGV_OK = 0
 NPHI, NA, NV, NDOF = 4, 3, 3, 10
 NOBS, NOBS_PHASE = 11, 14
+NOALLOC_MAX_N = 128
 
 PV2HBSPLIT, PV2HBSPLIT_NODIFFUSE, PV2HBSPLIT_ONLYDIFFUSE = 0, 1, 2
 IDEAL_PV2, EULER_LANGEVIN_HB, CHARGE_HB, MODELA_EM = 3, 4, 5, 6
@@ -78,6 +79,7 @@ SIGNATURES = [
     ("lgv_timing_read", C.c_int, [_H, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     ("lgv_debug_flags", C.c_int, [_H, C.c_int]),
     ("lgv_get_flags", C.c_int, [_H, C.c_void_p]),
+    ("lgv_measure_aos_noalloc", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
 ]
 
 _lib = None

@@ -320,6 +320,9 @@ int copy_injected(double **dst, const double *src, size_t n) {
 
 }  // namespace
 
+// Lets other translation units of the library report through lgv_last_error().
+void lgv_internal_set_error(const char *msg) { g_last_error = msg ? msg : ""; }
+
 // ============================================================================
 extern "C" {
 

@@ -75,5 +75,10 @@ cudaError_t launch_energy(Fields f, int N, double H, double inv2chi_half, double
 size_t measure_size(int N);
 size_t measure_scratch_doubles(int N);
 cudaError_t launch_measure(Fields f, int N, double *scratch, double *dev_out, cudaStream_t st);
+// Pieces of the measurement for a lattice in host-order AoS layout (device
+// memory): the observable sums into T[25][N][N] and U[25][N][N], then walls,
+// OAverage, DFT and vev rotation into dev_out (lgv.h packing).
+cudaError_t launch_measure_sums_aos(const double *aos, int N, double *T, double *U, cudaStream_t st);
+cudaError_t launch_measure_finish(const double *T, const double *U, int N, double *dev_out, cudaStream_t st);
 
 }  // namespace lgv

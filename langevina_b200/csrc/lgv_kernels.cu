@@ -765,6 +765,52 @@ __global__ void meas_rotate_kernel(int N, MeasOut mo) {
   put(13, re(10, kk), im(10, kk));
 }
 
+// Sums of the 25 observables over a lattice given in the host-order AoS layout
+// u[k][j][i][10] (used by the allocation-free measurement entry point).
+// T[o][k][i] = sum_j obs(i, j, k)
+__global__ void meas_sum_j_aos_kernel(const double *__restrict__ aos, int N, double *T) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)N * N) return;
+  const int i = (int)(t % N), k = (int)(t / N);
+  double acc[kNObs];
+#pragma unroll
+  for (int o = 0; o < kNObs; ++o) acc[o] = 0;
+  for (int j = 0; j < N; ++j) {
+    const double *src = aos + (((long long)k * N + j) * N + i) * 10;
+    double s[10], ob[kNObs];
+#pragma unroll
+    for (int L = 0; L < 10; ++L) s[L] = src[L];
+    site_obs(s, ob);
+#pragma unroll
+    for (int o = 0; o < kNObs; ++o) acc[o] += ob[o];
+  }
+  const long long NN = (long long)N * N;
+#pragma unroll
+  for (int o = 0; o < kNObs; ++o) T[o * NN + (long long)k * N + i] = acc[o];
+}
+
+// U[o][j][i] = sum_k obs(i, j, k)
+__global__ void meas_sum_k_aos_kernel(const double *__restrict__ aos, int N, double *U) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)N * N) return;
+  const int i = (int)(t % N), j = (int)(t / N);
+  double acc[kNObs];
+#pragma unroll
+  for (int o = 0; o < kNObs; ++o) acc[o] = 0;
+  for (int k = 0; k < N; ++k) {
+    const double *src = aos + (((long long)k * N + j) * N + i) * 10;
+    double s[10], ob[kNObs];
+#pragma unroll
+    for (int L = 0; L < 10; ++L) s[L] = src[L];
+    site_obs(s, ob);
+#pragma unroll
+    for (int o = 0; o < kNObs; ++o) acc[o] += ob[o];
+  }
+  const long long NN = (long long)N * N;
+#pragma unroll
+  for (int o = 0; o < kNObs; ++o) U[o * NN + (long long)j * N + i] = acc[o];
+}
+
 inline unsigned nblocks(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
 
 }  // namespace
@@ -877,6 +923,23 @@ cudaError_t launch_measure(Fields f, int N, double *scratch, double *dev_out, cu
   double *T = scratch, *U = scratch + (size_t)kNObs * NN;
   meas_sum_j_kernel<<<nblocks(NN, 128), 128, 0, st>>>(f, g, T);
   meas_sum_k_kernel<<<nblocks(NN, 128), 128, 0, st>>>(f, g, U);
+  const MeasOut mo = meas_layout(dev_out, N);
+  meas_walls_kernel<<<nblocks(3LL * kNObs * N, 128), 128, 0, st>>>(T, U, N, mo);
+  const int NK = N / 2 + 1;
+  meas_dft_kernel<<<nblocks(3LL * kNObs * NK, 128), 128, 0, st>>>(N, mo);
+  meas_rotate_kernel<<<nblocks(3LL * NK, 128), 128, 0, st>>>(N, mo);
+  return cudaGetLastError();
+}
+
+
+cudaError_t launch_measure_sums_aos(const double *aos, int N, double *T, double *U, cudaStream_t st) {
+  const long long NN = (long long)N * N;
+  meas_sum_j_aos_kernel<<<nblocks(NN, 128), 128, 0, st>>>(aos, N, T);
+  meas_sum_k_aos_kernel<<<nblocks(NN, 128), 128, 0, st>>>(aos, N, U);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_measure_finish(const double *T, const double *U, int N, double *dev_out, cudaStream_t st) {
   const MeasOut mo = meas_layout(dev_out, N);
   meas_walls_kernel<<<nblocks(3LL * kNObs * N, 128), 128, 0, st>>>(T, U, N, mo);
   const int NK = N / 2 + 1;
