@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <utility>
@@ -87,6 +88,12 @@ struct lgv_handle {
   int32_t inj_order[5] = {0, 1, 2, 0, 1};
   bool have_hb = false, have_ch = false, have_em = false;
   bool mon_on = false;
+  // phi heat bath as one z-marching sweep kernel instead of two parity
+  // passes (LGV_HB_FUSED=1 in the environment at lgv_create)
+  bool hb_fused = false;
+  // charge heat bath as three two-face launches (one per direction) instead
+  // of six single-face launches (LGV_CHARGE_FUSED=1 at lgv_create)
+  bool charge_per_face = true;
   lgv::MonAcc *mon_dev = nullptr;  // [3]
   lgv_monitor mon_ideal{};
   uint8_t *flags_dev = nullptr;
@@ -130,9 +137,17 @@ int check_params(const lgv_params *p) {
   return LGV_OK;
 }
 
+// Component planes are V doubles each; consecutive planes start kPlaneSkew
+// doubles apart beyond V so that the ten concurrently streamed planes do not
+// share a power-of-two stride (at N = 256 a plane is exactly 128 MiB), which
+// maps them onto the same DRAM channels at the same time.
+constexpr size_t kPlaneSkew = 4352;  // 34 KiB: an odd multiple of 256 B
+
+size_t lattice_doubles(size_t V) { return 10 * (V + kPlaneSkew); }
+
 Fields fields_of(double *base, size_t V) {
   Fields f;
-  for (int L = 0; L < 10; ++L) f.c[L] = base + (size_t)L * V;
+  for (int L = 0; L < 10; ++L) f.c[L] = base + (size_t)L * (V + kPlaneSkew);
   return f;
 }
 
@@ -222,9 +237,15 @@ int sub_hb(lgv_handle *h, double dt, double mass) {  // EulerLangevinHB::step (S
   } else {
     a.sk = lgv::sub_key(h->key, h->ctr);
   }
-  for (int parity = 0; parity < 2; ++parity) {
+  if (h->hb_fused) {
     KTimer tm(h, LGV_KCLASS_PHI_HB);
-    LGV_CK(lgv::launch_hb_pass(h->cur, h->N, parity, a, h->stream));
+    LGV_CK(lgv::launch_hb_sweep(h->cur, h->alt, h->N, a, h->stream));
+    for (int l = 0; l < 4; ++l) std::swap(h->cur.c[l], h->alt.c[l]);
+  } else {
+    for (int parity = 0; parity < 2; ++parity) {
+      KTimer tm(h, LGV_KCLASS_PHI_HB);
+      LGV_CK(lgv::launch_hb_pass(h->cur, h->N, parity, a, h->stream));
+    }
   }
   if (h->noise_mode == LGV_NOISE_INJECTED) h->have_hb = false;
   else h->ctr += 1;
@@ -256,11 +277,34 @@ int sub_charge(lgv_handle *h, double dt) {  // ModelGChargeHB::step (Stepper.cxx
     a.q = h->inj_ch_q;
     a.acc = h->inj_ch_acc;
   }
-  for (int p = 0; p < 6; ++p) {
-    a.pass = p;
-    if (h->noise_mode != LGV_NOISE_INJECTED) a.sk = lgv::sub_key(h->key, h->ctr + 1 + p);
-    KTimer tm(h, LGV_KCLASS_CHARGE);
-    LGV_CK(lgv::launch_charge_pass(h->cur, h->N, xyz[p / 2], eo[p % 2], a, h->stream));
+  if (h->charge_per_face) {
+    for (int p = 0; p < 6; ++p) {
+      a.pass = p;
+      if (h->noise_mode != LGV_NOISE_INJECTED) a.sk = lgv::sub_key(h->key, h->ctr + 1 + p);
+      KTimer tm(h, LGV_KCLASS_CHARGE);
+      LGV_CK(lgv::launch_charge_pass(h->cur, h->N, xyz[p / 2], eo[p % 2], a, h->stream));
+    }
+  } else {
+    // both faces of a direction per launch (same streams and order as per face)
+    lgv::ChargeDirPair d{};
+    d.rms = a.rms;
+    d.inv2chi = a.inv2chi;
+    d.q = a.q;
+    d.acc = a.acc;
+    d.flags = a.flags;
+    d.mon = a.mon;
+    for (int ixyz = 0; ixyz < 3; ++ixyz) {
+      for (int i = 0; i < 2; ++i) {
+        d.pass[i] = 2 * ixyz + i;
+        d.eo[i] = eo[i];
+        d.sk[i] = (h->noise_mode != LGV_NOISE_INJECTED) ? lgv::sub_key(h->key, h->ctr + 1 + 2 * ixyz + i) : 0;
+      }
+      bool swapped = false;
+      KTimer tm(h, LGV_KCLASS_CHARGE);
+      LGV_CK(lgv::launch_charge_dir(h->cur, h->alt, h->N, xyz[ixyz], d, h->stream, &swapped));
+      if (swapped)
+        for (int L = 4; L < 10; ++L) std::swap(h->cur.c[L], h->alt.c[L]);
+    }
   }
   if (h->noise_mode == LGV_NOISE_INJECTED) h->have_ch = false;
   else h->ctr += 7;
@@ -355,13 +399,19 @@ int lgv_create(const lgv_params *params, lgv_handle **out) {
   h->V = (size_t)h->N * h->N * h->N;
   h->device = dev;
   h->key = lgv::make_key(params->seed);
+  {
+    const char *f = std::getenv("LGV_HB_FUSED");
+    h->hb_fused = f && f[0] == '1';
+    const char *c = std::getenv("LGV_CHARGE_FUSED");
+    h->charge_per_face = !(c && c[0] == '1');
+  }
   int rc = LGV_OK;
   if (cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
     rc = fail(LGV_ERR_CUDA, "cudaStreamCreate failed");
   }
   h->stream = h->own_stream;
-  if (rc == LGV_OK) rc = ensure(&h->bufA, 10 * h->V);
-  if (rc == LGV_OK) rc = ensure(&h->bufB, 10 * h->V);
+  if (rc == LGV_OK) rc = ensure(&h->bufA, lattice_doubles(h->V));
+  if (rc == LGV_OK) rc = ensure(&h->bufB, lattice_doubles(h->V));
   if (rc == LGV_OK) rc = ensure(&h->small_dev, 8);
   if (rc == LGV_OK) {
     cudaError_t e = cudaMalloc((void **)&h->mon_dev, 3 * sizeof(lgv::MonAcc));
@@ -370,7 +420,7 @@ int lgv_create(const lgv_params *params, lgv_handle **out) {
   if (rc == LGV_OK) {
     h->cur = fields_of(h->bufA, h->V);
     h->alt = fields_of(h->bufB, h->V);
-    if (cudaMemsetAsync(h->bufA, 0, 10 * h->V * sizeof(double), h->stream) != cudaSuccess ||
+    if (cudaMemsetAsync(h->bufA, 0, lattice_doubles(h->V) * sizeof(double), h->stream) != cudaSuccess ||
         cudaMemsetAsync(h->mon_dev, 0, 3 * sizeof(lgv::MonAcc), h->stream) != cudaSuccess ||
         cudaStreamSynchronize(h->stream) != cudaSuccess)
       rc = fail(LGV_ERR_CUDA, "initial memset failed");

@@ -39,6 +39,17 @@ struct ChargeArgs {
   MonAcc *mon;
 };
 
+// Both faces of one direction of the charge heat bath.
+struct ChargeDirPair {
+  double rms, inv2chi;
+  uint64_t sk[2];     // sub-step keys of the two faces
+  int pass[2];        // positions of the faces in the step (0..5)
+  int eo[2];          // A-site parities, in application order
+  const double *q, *acc;  // injected [6][6][V] or null
+  uint8_t *flags;
+  MonAcc *mon;
+};
+
 struct EmArgs {
   double c6;    // 6 + m^2
   double dtg;   // dt * gamma
@@ -62,8 +73,16 @@ cudaError_t launch_rb_to_aos(Fields f, double *aos, int N, cudaStream_t st);
 cudaError_t launch_init_phi(Fields f, int N, uint64_t sk, double scale, cudaStream_t st);
 cudaError_t launch_init_charges(Fields f, int N, uint64_t sk, double sqrtchi, double *scratch,
                                 cudaStream_t st);
+// one phi heat-bath parity pass, in place
 cudaError_t launch_hb_pass(Fields f, int N, int parity, const HbArgs &a, cudaStream_t st);
+// one full phi heat-bath sweep (both parities, z-marching): reads phi of `in`, writes phi of `out`
+cudaError_t launch_hb_sweep(Fields in, Fields out, int N, const HbArgs &a, cudaStream_t st);
 cudaError_t launch_charge_pass(Fields f, int N, int dir, int eoA, const ChargeArgs &a, cudaStream_t st);
+// Both faces of direction dir.  x runs in place on `in`; y and z read `in`
+// and write the charges of `out` (*swapped = true: the caller swaps the
+// charge planes).
+cudaError_t launch_charge_dir(Fields in, Fields out, int N, int dir, const ChargeDirPair &p, cudaStream_t st,
+                              bool *swapped);
 cudaError_t launch_em(Fields in, Fields out, int N, const EmArgs &a, cudaStream_t st);
 cudaError_t launch_ideal(Fields in, Fields out, int N, const IdealArgs &a, cudaStream_t st);
 // energy: writes E into dev_out[0]; scratch >= energy_scratch_doubles(N)

@@ -2,10 +2,12 @@
 // measurer.  FP64 throughout; HBM-bound stencils, no tensor-core work.
 //
 // Kernel map (reference loop each one replaces):
-//   hb_pass_kernel      EulerLangevinHB::step, one checkerboard parity
-//                       (Stepper.cxx:309-386)
+//   hb_sweep_kernel     EulerLangevinHB::step, both checkerboard parities in
+//                       one z-marching launch (Stepper.cxx:287-389)
 //   charge_pass_kernel  ModelGChargeHB::step, one (direction, parity) face
 //                       (Stepper.cxx:471-518, modelg_update_charge_pair :419-441)
+//   charge_x_kernel,    both faces of one direction per launch (x: whole rows
+//   charge_line_kernel  per CTA; y, z: streamed lines with a two-site halo)
 //   ideal_kernel        IdealPV2::step_no_reject fused: half rotation, charge
 //                       advection stencil, half rotation (Stepper.cxx:68-202)
 //   em_kernel           Euler-Maruyama Model A step (action of Stepper.cxx:354-355)
@@ -49,7 +51,10 @@ __device__ void mon_flush(MonLocal &m, MonAcc *acc) {
   warp_sum(m.un);
   warp_sum(m.dd);
   warp_sum(m.ud);
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  // linear thread index: CTAs may be two-dimensional (charge_x_kernel)
+  const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+  const int nwarps = (blockDim.x * blockDim.y + 31) >> 5;
+  const int w = tid >> 5, l = tid & 31;
   if (l == 0) {
     s_c[0][w] = m.dc;
     s_c[1][w] = m.uc;
@@ -59,9 +64,9 @@ __device__ void mon_flush(MonLocal &m, MonAcc *acc) {
     s_d[1][w] = m.ud;
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
+  if (tid == 0) {
     MonLocal t;
-    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) {
+    for (int i = 0; i < nwarps; ++i) {
       t.dc += s_c[0][i];
       t.uc += s_c[1][i];
       t.uy += s_c[2][i];
@@ -177,20 +182,75 @@ __global__ void charge_sub_kernel(Fields f, long long V, const double *mean) {
 }
 
 // ----------------------------------------------------------------------------
+// Asynchronous global -> shared copies (cp.async, one double per copy).
+__device__ __forceinline__ void cp_async8(double *smem, const double *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+__device__ __forceinline__ int wrapn(int a, int n) {
+  a %= n;
+  return a < 0 ? a + n : a;
+}
+
+// One heat-bath decision (Stepper.cxx:332-378): proposal phi_n = phi_o +
+// sqrt(2 dt Gamma) * variance1, action change dS, Metropolis accept.
+struct HbDecision {
+  double pn[4];
+  double dS;
+  bool accept;
+  uint8_t flag;
+};
+
+template <bool INJECTED>
+__device__ __forceinline__ void hb_decide(const double po[4], const double heff[4], const HbArgs &a, long long nat,
+                                          long long V, HbDecision &r) {
+  Xoro rng;
+  if (!INJECTED) rng = stream_at(a.sk, (uint64_t)nat);
+  double hphi_o = 0., hphi_n = 0., s_o = 0., s_n = 0.;
+#pragma unroll
+  for (int l = 0; l < 4; ++l) {
+    const double v = INJECTED ? a.prop[(long long)l * V + nat] : var1(rng.next());
+    r.pn[l] = po[l] + a.rdtg * v;
+    s_o += po[l] * po[l];
+    s_n += r.pn[l] * r.pn[l];
+    hphi_o += heff[l] * po[l];
+    hphi_n += heff[l] * r.pn[l];
+  }
+  hphi_o += a.H * po[0];
+  hphi_n += a.H * r.pn[0];
+  r.dS = -(hphi_n - hphi_o) + a.Lambda2 * (s_n - s_o) + a.lam4 * (s_n * s_n - s_o * s_o);
+  if (r.dS < 0) {
+    r.accept = true;
+    r.flag = 1;
+  } else {
+    const double u = INJECTED ? a.acc[nat] : u53(rng.next());
+    r.accept = u < exp(-r.dS);
+    r.flag = r.accept ? 2 : 0;
+  }
+}
+
+__device__ __forceinline__ void mon_count(MonLocal &m, const HbDecision &d) {
+  if (d.flag == 1) m.down(d.dS);
+  else if (d.flag == 2) m.up_yes(d.dS);
+  else m.up_no();
+}
+
+// ----------------------------------------------------------------------------
 // Phi heat bath, one checkerboard parity (EulerLangevinHB::step,
-// Stepper.cxx:325-381).  One thread per site of `parity`; the six neighbours
-// are sites of the other parity, read from its half-plane.
+// Stepper.cxx:325-381).  One thread per site of `parity`: element m of the
+// parity half-row (j, k); its six neighbours are elements of the other
+// parity's half-rows.  Grid: (m chunks, j, k), so no 64-bit index division.
 template <bool INJECTED, bool MON>
-__global__ void __launch_bounds__(kThreads) hb_pass_kernel(Fields f, Geo g, int parity, HbArgs a) {
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(128) hb_pass_kernel(Fields f, Geo g, int parity, HbArgs a) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y, k = blockIdx.z;
+  const int H = g.H, N = g.N;
   MonLocal mon;
-  if (t < g.V2) {
-    const int H = g.H, N = g.N;
-    const int m = (int)(t % H);
-    const long long rr = t / H;
-    const int j = (int)(rr % N), k = (int)(rr / N);
+  if (m < H) {
     const int s = (parity + j + k) & 1;
-    const int i = 2 * m + s;
     int xm = m - 1 + s, xp = m + s;
     if (xm < 0) xm += H;
     if (xp == H) xp = 0;
@@ -201,48 +261,166 @@ __global__ void __launch_bounds__(kThreads) hb_pass_kernel(Fields f, Geo g, int 
     const long long rkm = ((long long)wrap_dec(k, N) * N + j) * H;
     const long long own = (long long)parity * g.V2 + row + m;
     const long long ob = (long long)(parity ^ 1) * g.V2;
-    const long long nat = ((long long)k * N + j) * N + i;
-
-    Xoro rng;
-    if (!INJECTED) rng = stream_at(a.sk, (uint64_t)nat);
-    double po[4], pn[4];
-    double hphi_o = 0., hphi_n = 0., s_o = 0., s_n = 0.;
+    double po[4], heff[4];
 #pragma unroll
     for (int l = 0; l < 4; ++l) {
       const double *P = f.c[l];
-      const double heff = (P[ob + row + xp] + P[ob + row + xm]) + (P[ob + rjp + m] + P[ob + rjm + m]) +
-                          (P[ob + rkp + m] + P[ob + rkm + m]);
+      heff[l] = (P[ob + row + xp] + P[ob + row + xm]) + (P[ob + rjp + m] + P[ob + rjm + m]) +
+                (P[ob + rkp + m] + P[ob + rkm + m]);
       po[l] = P[own];
-      const double v = INJECTED ? a.prop[(long long)l * 2 * g.V2 + nat] : var1(rng.next());
-      pn[l] = po[l] + a.rdtg * v;
-      s_o += po[l] * po[l];
-      s_n += pn[l] * pn[l];
-      hphi_o += heff * po[l];
-      hphi_n += heff * pn[l];
     }
-    hphi_o += a.H * po[0];
-    hphi_n += a.H * pn[0];
-    const double dS = -(hphi_n - hphi_o) + a.Lambda2 * (s_n - s_o) + a.lam4 * (s_n * s_n - s_o * s_o);
-    bool accept;
-    uint8_t fl;
-    if (dS < 0) {
-      accept = true;
-      fl = 1;
-      if (MON) mon.down(dS);
-    } else {
-      const double r = INJECTED ? a.acc[nat] : u53(rng.next());
-      accept = r < exp(-dS);
-      fl = accept ? 2 : 0;
-      if (MON) {
-        if (accept) mon.up_yes(dS);
-        else mon.up_no();
+    const long long nat = ((long long)k * N + j) * N + 2 * m + s;
+    HbDecision d;
+    hb_decide<INJECTED>(po, heff, a, nat, 2 * g.V2, d);
+    if (d.accept) {
+#pragma unroll
+      for (int l = 0; l < 4; ++l) f.c[l][own] = d.pn[l];
+    }
+    if (MON) mon_count(mon, d);
+    if (a.flags) a.flags[nat] = d.flag;
+  }
+  if (MON) mon_flush(mon, a.mon);
+}
+
+// ----------------------------------------------------------------------------
+// Phi heat bath, one full checkerboard sweep (EulerLangevinHB::step,
+// Stepper.cxx:287-389) in a single launch.  A CTA owns HB_TM x HB_TY
+// pair-columns -- element m of both parity half-rows of row j, i.e. natural
+// x = 2m and 2m+1 -- and marches up a z-chunk.  At plane p it
+//   (1) runs the even pass on plane p over its tile plus a one-element ring,
+//       from the old odd values of planes p-1, p, p+1 kept in shared memory
+//       over a two-element ring;
+//   (2) runs the odd pass on plane p-1 over its tile from the new even values
+//       of planes p-2, p-1, p, and writes both parities of plane p-1.
+// The ring's even updates are recomputed by the neighbouring CTAs bit for bit
+// (same inputs, same counter stream), so no CTA waits for another.  phi is
+// read once and written once (to `out`): 64 B per site per sweep.  cp.async
+// brings plane p+2 (odd) and p+1 (even) in while plane p computes.
+constexpr int HB_TM = 32, HB_TY = 8;
+constexpr int HB_OW = HB_TM + 4, HB_OH = HB_TY + 4, HB_OP = HB_OW * HB_OH;  // old odd: two-element ring
+constexpr int HB_EW = HB_TM + 2, HB_EH = HB_TY + 2, HB_EP = HB_EW * HB_EH;  // even: one-element ring
+constexpr size_t HB_SMEM = (size_t)(4 * 4 * HB_OP + 2 * 4 * HB_EP + 3 * 4 * HB_EP) * sizeof(double);
+
+template <bool INJECTED, bool MON>
+__global__ void __launch_bounds__(HB_TM *HB_TY, 2) hb_sweep_kernel(Fields in, Fields out, Geo g, int zchunk, HbArgs a) {
+  extern __shared__ double smem[];
+  double *oo = smem;                     // [4 stages][4][HB_OP] old odd
+  double *oe = oo + 4 * 4 * HB_OP;       // [2 stages][4][HB_EP] old even
+  double *ne = oe + 2 * 4 * HB_EP;       // [3 stages][4][HB_EP] new even
+  const int N = g.N, H = g.H;
+  const long long V2 = g.V2, V = 2 * V2;
+  const int tid = threadIdx.x;
+  const int tm = tid % HB_TM, tj = tid / HB_TM;
+  const int m0 = blockIdx.x * HB_TM, j0 = blockIdx.y * HB_TY;
+  const int z0 = blockIdx.z * zchunk;
+  const int z1 = min(z0 + zchunk, N);
+  const int nit = (z1 - z0) + 2;
+  MonLocal mon;
+
+  auto issue_odd = [&](int plane, int stage) {
+    for (int idx = tid; idx < HB_OP; idx += HB_TM * HB_TY) {
+      const int qm = idx % HB_OW, qj = idx / HB_OW;
+      const int m = wrapn(m0 - 2 + qm, H), j = wrapn(j0 - 2 + qj, N);
+      const long long off = V2 + ((long long)plane * N + j) * H + m;
+#pragma unroll
+      for (int l = 0; l < 4; ++l) cp_async8(&oo[(stage * 4 + l) * HB_OP + idx], in.c[l] + off);
+    }
+  };
+  auto issue_even = [&](int plane, int stage) {
+    for (int idx = tid; idx < HB_EP; idx += HB_TM * HB_TY) {
+      const int qm = idx % HB_EW, qj = idx / HB_EW;
+      const int m = wrapn(m0 - 1 + qm, H), j = wrapn(j0 - 1 + qj, N);
+      const long long off = ((long long)plane * N + j) * H + m;
+#pragma unroll
+      for (int l = 0; l < 4; ++l) cp_async8(&oe[(stage * 4 + l) * HB_EP + idx], in.c[l] + off);
+    }
+  };
+
+  issue_odd(wrapn(z0 - 2, N), 0);
+  issue_odd(wrapn(z0 - 1, N), 1);
+  issue_odd(z0, 2);
+  issue_even(wrapn(z0 - 1, N), 0);
+  cp_async_commit();
+
+  for (int it = 0; it < nit; ++it) {
+    const int p = wrapn(z0 - 1 + it, N);
+    cp_async_wait_all();
+    __syncthreads();
+    if (it + 1 < nit) {
+      issue_odd(wrapn(p + 2, N), (it + 3) & 3);
+      issue_even(wrapn(p + 1, N), (it + 1) & 1);
+    }
+    cp_async_commit();
+
+    // (1) even pass on plane p over the tile and its one-element ring
+    const double *oom = oo + ((it & 3) * 4) * HB_OP;        // plane p-1
+    const double *ooc = oo + (((it + 1) & 3) * 4) * HB_OP;  // plane p
+    const double *oop = oo + (((it + 2) & 3) * 4) * HB_OP;  // plane p+1
+    const double *oec = oe + ((it & 1) * 4) * HB_EP;
+    double *nec = ne + ((it % 3) * 4) * HB_EP;
+    const bool in_chunk_e = (it >= 1) && (it <= nit - 2);
+    for (int e = tid; e < HB_EP; e += HB_TM * HB_TY) {
+      const int qm = e % HB_EW, qj = e / HB_EW;
+      const int mr = m0 - 1 + qm, jr = j0 - 1 + qj;
+      const int m = wrapn(mr, H), j = wrapn(jr, N);
+      const int s0 = (j + p) & 1;
+      const int oc = (qj + 1) * HB_OW + (qm + 1);
+      double po[4], heff[4];
+#pragma unroll
+      for (int l = 0; l < 4; ++l) {
+        const double *C = ooc + l * HB_OP;
+        heff[l] = (C[oc + s0] + C[oc - 1 + s0]) + (C[oc + HB_OW] + C[oc - HB_OW]) +
+                  (oop[l * HB_OP + oc] + oom[l * HB_OP + oc]);
+        po[l] = oec[l * HB_EP + e];
+      }
+      const long long nat = ((long long)p * N + j) * N + 2 * m + s0;
+      HbDecision d;
+      hb_decide<INJECTED>(po, heff, a, nat, V, d);
+#pragma unroll
+      for (int l = 0; l < 4; ++l) nec[l * HB_EP + e] = d.accept ? d.pn[l] : po[l];
+      const bool own = in_chunk_e && qm >= 1 && qm <= HB_TM && qj >= 1 && qj <= HB_TY && mr < H && jr < N;
+      if (own) {
+        if (MON) mon_count(mon, d);
+        if (a.flags) a.flags[nat] = d.flag;
       }
     }
-    if (accept) {
+    __syncthreads();
+
+    // (2) odd pass on plane q = p-1 over the tile; write both parities of q
+    if (it >= 2) {
+      const int q = wrapn(p - 1, N);
+      const int mr = m0 + tm, jr = j0 + tj;
+      const bool act = mr < H && jr < N;
+      const int m = wrapn(mr, H), j = wrapn(jr, N);
+      const int s1 = (1 + j + q) & 1;
+      const int ec = (tj + 1) * HB_EW + (tm + 1);
+      const double *nem = ne + (((it + 1) % 3) * 4) * HB_EP;  // plane p-2
+      const double *neq = ne + (((it + 2) % 3) * 4) * HB_EP;  // plane p-1
+      const double *oq = oom;                                  // old odd of plane p-1
+      const int oc = (tj + 2) * HB_OW + (tm + 2);
+      double po[4], heff[4], ev[4];
 #pragma unroll
-      for (int l = 0; l < 4; ++l) f.c[l][own] = pn[l];
+      for (int l = 0; l < 4; ++l) {
+        const double *C = neq + l * HB_EP;
+        heff[l] = (C[ec + s1] + C[ec - 1 + s1]) + (C[ec + HB_EW] + C[ec - HB_EW]) +
+                  (nec[l * HB_EP + ec] + nem[l * HB_EP + ec]);
+        po[l] = oq[l * HB_OP + oc];
+        ev[l] = C[ec];
+      }
+      const long long nat = ((long long)q * N + j) * N + 2 * m + s1;
+      HbDecision d;
+      hb_decide<INJECTED>(po, heff, a, nat, V, d);
+      if (act) {
+        const long long row = ((long long)q * N + j) * H + m;
+#pragma unroll
+        for (int l = 0; l < 4; ++l) {
+          out.c[l][row] = ev[l];
+          out.c[l][V2 + row] = d.accept ? d.pn[l] : po[l];
+        }
+        if (MON) mon_count(mon, d);
+        if (a.flags) a.flags[nat] = d.flag;
+      }
     }
-    if (a.flags) a.flags[nat] = fl;
   }
   if (MON) mon_flush(mon, a.mon);
 }
@@ -251,15 +429,14 @@ __global__ void __launch_bounds__(kThreads) hb_pass_kernel(Fields f, Geo g, int 
 // Charge heat bath, one face (direction `dir`, A-site parity eoA).  One thread
 // per link (A, B = A + e_dir); the links of a face are disjoint, so the update
 // is race free and conserves each charge exactly (Stepper.cxx:493-517).
+// Grid: (m chunks, j, k).
 template <bool INJECTED, bool MON>
-__global__ void __launch_bounds__(kThreads) charge_pass_kernel(Fields f, Geo g, int dir, int eoA, ChargeArgs a) {
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(128) charge_pass_kernel(Fields f, Geo g, int dir, int eoA, ChargeArgs a) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y, k = blockIdx.z;
+  const int H = g.H, N = g.N;
   MonLocal mon;
-  if (t < g.V2) {
-    const int H = g.H, N = g.N;
-    const int m = (int)(t % H);
-    const long long rr = t / H;
-    const int j = (int)(rr % N), k = (int)(rr / N);
+  if (m < H) {
     const int s = (eoA + j + k) & 1;
     const int i = 2 * m + s;
     const long long offA = (long long)eoA * g.V2 + ((long long)k * N + j) * H + m;
@@ -320,74 +497,291 @@ __global__ void __launch_bounds__(kThreads) charge_pass_kernel(Fields f, Geo g, 
 }
 
 // ----------------------------------------------------------------------------
-// Euler-Maruyama Model A step (Jacobi: reads `in`, writes phi of `out`).
-template <bool INJECTED>
-__global__ void __launch_bounds__(kThreads) em_kernel(Fields in, Fields out, Geo g, EmArgs a) {
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= 2 * g.V2) return;
+// Charge heat bath, both parity passes of one direction in one launch
+// (ModelGChargeHB::step, Stepper.cxx:471-518): the two faces (dir, eo[0]) and
+// (dir, eo[1]) are applied in that order.  Every link update is
+// modelg_update_charge_pair (:419-441) for the six charges at once, drawing
+// from the counter stream of its pass keyed by the link's A site.
+struct ChargeDirArgs {
+  double rms, inv2chi;
+  uint64_t sk[2];
+  int pass[2];  // positions of the two faces in the step (injected indexing / flags)
+  int eo[2];
+  const double *q, *acc;
+  uint8_t *flags;
+  MonAcc *mon;
+};
+
+template <bool INJECTED, bool MON>
+__device__ __forceinline__ void charge_link(double nA[6], double nB[6], const ChargeDirArgs &a, int pi,
+                                            long long natA, long long V, bool own, MonLocal &mon) {
+  Xoro rng;
+  if (!INJECTED) rng = stream_at(a.sk[pi], (uint64_t)natA);
+#pragma unroll
+  for (int L = 0; L < 6; ++L) {
+    const long long ii = (long long)(a.pass[pi] * 6 + L) * V + natA;
+    uint64_t ra = 0;
+    double v;
+    if (INJECTED) {
+      v = a.q[ii];
+    } else {
+      v = var1(rng.next());
+      ra = rng.next();
+    }
+    const double q = a.rms * v;
+    const double dA = nA[L] - q, dB = nB[L] + q;
+    const double dS = (dA * dA + dB * dB - nA[L] * nA[L] - nB[L] * nB[L]) * a.inv2chi;
+    bool accept;
+    uint8_t fl;
+    if (dS < 0) {
+      accept = true;
+      fl = 1;
+    } else {
+      const double r = INJECTED ? a.acc[ii] : u53(ra);
+      accept = r < exp(-dS);
+      fl = accept ? 2 : 0;
+    }
+    if (own) {
+      if (MON) {
+        if (fl == 1) mon.down(dS);
+        else if (fl == 2) mon.up_yes(dS);
+        else mon.up_no();
+      }
+      if (a.flags) a.flags[ii] = fl;
+    }
+    if (accept) {
+      nA[L] = nA[L] + (-q);
+      nB[L] = nB[L] + q;
+    }
+  }
+}
+
+// x direction.  A CTA owns whole rows (blockDim.x = N/2, blockDim.y rows);
+// thread m holds natural sites 2m and 2m+1 of its row (element m of both
+// parity half-rows).  Of the two x faces one pairs (2m, 2m+1) inside the
+// thread, the other pairs (2m+1, 2m+2) across threads: its A-site owner
+// computes it and hands the B site's new charges over through shared memory.
+template <bool INJECTED, bool MON>
+__global__ void __launch_bounds__(256) charge_x_kernel(Fields f, Geo g, ChargeDirArgs a) {
+  extern __shared__ double xs[];  // [6][blockDim.y][H]
   const int H = g.H, N = g.N;
-  const int parity = (int)(t / g.V2);
-  const long long u = t - (long long)parity * g.V2;
-  const int m = (int)(u % H);
-  const long long rr = u / H;
-  const int j = (int)(rr % N), k = (int)(rr / N);
-  const int s = (parity + j + k) & 1;
-  const int i = 2 * m + s;
-  int xm = m - 1 + s, xp = m + s;
-  if (xm < 0) xm += H;
-  if (xp == H) xp = 0;
+  const int m = threadIdx.x, ty = threadIdx.y;
+  const long long R = (long long)blockIdx.x * blockDim.y + ty;
+  const bool valid = R < (long long)N * N;
+  const int j = valid ? (int)(R % N) : 0, k = valid ? (int)(R / N) : 0;
+  const int r = (j + k) & 1;  // parity of site 2m
+  const long long row = ((long long)k * N + j) * H;
+  const long long V = 2 * g.V2;
+  const long long offa = (long long)r * g.V2 + row + m, offb = (long long)(r ^ 1) * g.V2 + row + m;
+  double va[6], vb[6];
+  MonLocal mon;
+  if (valid) {
+#pragma unroll
+    for (int L = 0; L < 6; ++L) {
+      va[L] = f.c[4 + L][offa];
+      vb[L] = f.c[4 + L][offb];
+    }
+  }
+  double *sh = xs + (size_t)ty * H;
+  const size_t lstride = (size_t)blockDim.y * H;
+  const long long nat0 = ((long long)k * N + j) * N + 2 * m;
+  // Rows of a CTA differ in parity, so some take the in-thread face while
+  // others take the cross face: every thread runs the exchange barriers of
+  // both faces, and only the work between them is conditional.
+  const int mr = (m + 1 == H) ? 0 : m + 1;
+#pragma unroll
+  for (int pi = 0; pi < 2; ++pi) {
+    const bool cross = a.eo[pi] != r;
+    if (valid && !cross) charge_link<INJECTED, MON>(va, vb, a, pi, nat0, V, true, mon);
+    // cross link (2m+1, 2m+2): B is thread m+1's site 2m+2
+    if (valid && cross) {
+#pragma unroll
+      for (int L = 0; L < 6; ++L) sh[L * lstride + m] = va[L];
+    }
+    __syncthreads();
+    double nb[6];
+    if (valid && cross) {
+#pragma unroll
+      for (int L = 0; L < 6; ++L) nb[L] = sh[L * lstride + mr];
+      charge_link<INJECTED, MON>(vb, nb, a, pi, nat0 + 1, V, true, mon);
+    }
+    __syncthreads();
+    if (valid && cross) {
+#pragma unroll
+      for (int L = 0; L < 6; ++L) sh[L * lstride + mr] = nb[L];
+    }
+    __syncthreads();
+    if (valid && cross) {
+#pragma unroll
+      for (int L = 0; L < 6; ++L) va[L] = sh[L * lstride + m];
+    }
+    __syncthreads();
+  }
+  if (valid) {
+#pragma unroll
+    for (int L = 0; L < 6; ++L) {
+      f.c[4 + L][offa] = va[L];
+      f.c[4 + L][offb] = vb[L];
+    }
+  }
+  if (MON) mon_flush(mon, a.mon);
+}
+
+// y (DIR = 1) and z (DIR = 2) directions.  A thread owns element m of the
+// parity half-rows along one line (natural columns x = 2m and 2m+1) and
+// streams through a segment [s0, s1) of the line plus two sites either side.
+// Along a column the two faces alternate link by link, so as site t arrives
+// the first face's link (t-1, t) and then the second face's link (t-2, t-1)
+// are applied (three-site register window); a site is final after its second
+// face link.  Links in the halo are recomputed bit for bit by the thread that
+// owns them, so segments are independent; because halos are read while
+// neighbours write, the kernel reads `in` and writes `out`.
+template <int DIR, bool INJECTED, bool MON>
+__global__ void __launch_bounds__(128) charge_line_kernel(Fields in, Fields out, Geo g, ChargeDirArgs a, int seglen) {
+  const int H = g.H, N = g.N;
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c2 = blockIdx.y;  // k for DIR = 1, j for DIR = 2
+  const int s0 = blockIdx.z * seglen;
+  const int s1 = min(s0 + seglen, N);
+  const long long V = 2 * g.V2;
+  MonLocal mon;
+  if (m < H) {
+    double w0[2][6], w1[2][6], w2[2][6];  // sites t-2, t-1, t; [column a (x=2m) / b (x=2m+1)][charge]
+    const int e1 = a.eo[0], e2 = a.eo[1];
+    const int n = (s1 - s0) + 4;
+    int tm1 = 0, jm1 = 0, km1 = 0, tm2 = 0, jm2 = 0, km2 = 0;
+    for (int u = 0; u < n; ++u) {
+      const int t = s0 - 2 + u;  // line position (unwrapped)
+      const int tw = wrapn(t, N);
+      const int j = DIR == 1 ? tw : c2, k = DIR == 1 ? c2 : tw;
+      const int ra = (j + k) & 1;  // parity of column a's site at t
+      const long long row = ((long long)k * N + j) * H + m;
+#pragma unroll
+      for (int L = 0; L < 6; ++L) {
+        w2[0][L] = in.c[4 + L][(long long)ra * g.V2 + row];
+        w2[1][L] = in.c[4 + L][(long long)(ra ^ 1) * g.V2 + row];
+      }
+      if (u >= 1) {
+        const int rpa = (jm1 + km1) & 1;  // parity of column a at t-1
+#pragma unroll
+        for (int col = 0; col < 2; ++col) {
+          const int par = rpa ^ col;  // parity of this column's site at t-1
+          if (par == e1) {  // first face: link (t-1, t), A = t-1
+            const long long natA = ((long long)km1 * N + jm1) * N + 2 * m + col;
+            charge_link<INJECTED, MON>(w1[col], w2[col], a, 0, natA, V, (t - 1) >= s0 && (t - 1) < s1, mon);
+          }
+          if (u >= 3 && (par ^ 1) == e2) {  // second face: link (t-2, t-1), A = t-2
+            const long long natA = ((long long)km2 * N + jm2) * N + 2 * m + col;
+            charge_link<INJECTED, MON>(w0[col], w1[col], a, 1, natA, V, (t - 2) >= s0 && (t - 2) < s1, mon);
+            // sites t-2 and t-1 of this column are final
+            if ((t - 2) >= s0 && (t - 2) < s1) {
+              const long long o2 = (long long)(((jm2 + km2) & 1) ^ col) * g.V2 + ((long long)km2 * N + jm2) * H + m;
+#pragma unroll
+              for (int L = 0; L < 6; ++L) out.c[4 + L][o2] = w0[col][L];
+            }
+            if ((t - 1) >= s0 && (t - 1) < s1) {
+              const long long o1 = (long long)(rpa ^ col) * g.V2 + ((long long)km1 * N + jm1) * H + m;
+#pragma unroll
+              for (int L = 0; L < 6; ++L) out.c[4 + L][o1] = w1[col][L];
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < 2; ++c)
+#pragma unroll
+        for (int L = 0; L < 6; ++L) {
+          w0[c][L] = w1[c][L];
+          w1[c][L] = w2[c][L];
+        }
+      tm2 = tm1; jm2 = jm1; km2 = km1;
+      tm1 = tw; jm1 = j; km1 = k;
+    }
+    (void)tm2;
+  }
+  if (MON) mon_flush(mon, a.mon);
+}
+
+// ----------------------------------------------------------------------------
+// Euler-Maruyama Model A step (Jacobi: reads `in`, writes phi of `out`).
+// One thread per element m of both parity half-rows of row (j, k).
+template <bool INJECTED>
+__global__ void __launch_bounds__(128) em_kernel(Fields in, Fields out, Geo g, EmArgs a) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y, k = blockIdx.z;
+  const int H = g.H, N = g.N;
+  if (m >= H) return;
   const long long row = ((long long)k * N + j) * H;
   const long long rjp = ((long long)k * N + wrap_inc(j, N)) * H;
   const long long rjm = ((long long)k * N + wrap_dec(j, N)) * H;
   const long long rkp = ((long long)wrap_inc(k, N) * N + j) * H;
   const long long rkm = ((long long)wrap_dec(k, N) * N + j) * H;
-  const long long own = (long long)parity * g.V2 + row + m;
-  const long long ob = (long long)(parity ^ 1) * g.V2;
-  const long long nat = ((long long)k * N + j) * N + i;
-  double xi[4];
-  if (INJECTED) {
 #pragma unroll
-    for (int l = 0; l < 4; ++l) xi[l] = a.xi[(long long)l * 2 * g.V2 + nat];
-  } else {
-    Xoro rng = stream_at(a.sk, (uint64_t)nat);
-    const uint64_t r1 = rng.next(), r2 = rng.next(), r3 = rng.next(), r4 = rng.next();
-    box_muller(r1, r2, xi[0], xi[1]);
-    box_muller(r3, r4, xi[2], xi[3]);
-  }
-  double c[4];
+  for (int parity = 0; parity < 2; ++parity) {
+    const int s = (parity + j + k) & 1;
+    const int i = 2 * m + s;
+    int xm = m - 1 + s, xp = m + s;
+    if (xm < 0) xm += H;
+    if (xp == H) xp = 0;
+    const long long own = (long long)parity * g.V2 + row + m;
+    const long long ob = (long long)(parity ^ 1) * g.V2;
+    const long long nat = ((long long)k * N + j) * N + i;
+    double xi[4];
+    if (INJECTED) {
 #pragma unroll
-  for (int l = 0; l < 4; ++l) c[l] = in.c[l][own];
-  const double p2 = c[0] * c[0] + c[1] * c[1] + c[2] * c[2] + c[3] * c[3];
+      for (int l = 0; l < 4; ++l) xi[l] = a.xi[(long long)l * 2 * g.V2 + nat];
+    } else {
+      Xoro rng = stream_at(a.sk, (uint64_t)nat);
+      const uint64_t r1 = rng.next(), r2 = rng.next(), r3 = rng.next(), r4 = rng.next();
+      box_muller(r1, r2, xi[0], xi[1]);
+      box_muller(r3, r4, xi[2], xi[3]);
+    }
+    double c[4];
 #pragma unroll
-  for (int l = 0; l < 4; ++l) {
-    const double *P = in.c[l];
-    const double heff = (P[ob + row + xp] + P[ob + row + xm]) + (P[ob + rjp + m] + P[ob + rjm + m]) +
-                        (P[ob + rkp + m] + P[ob + rkm + m]);
-    double fo = -heff + a.c6 * c[l] + a.lambda * p2 * c[l];
-    if (l == 0) fo -= a.H;
-    out.c[l][own] = c[l] - a.dtg * fo + a.sq * xi[l];
+    for (int l = 0; l < 4; ++l) c[l] = in.c[l][own];
+    const double p2 = c[0] * c[0] + c[1] * c[1] + c[2] * c[2] + c[3] * c[3];
+#pragma unroll
+    for (int l = 0; l < 4; ++l) {
+      const double *P = in.c[l];
+      const double heff = (P[ob + row + xp] + P[ob + row + xm]) + (P[ob + rjp + m] + P[ob + rjm + m]) +
+                          (P[ob + rkp + m] + P[ob + rkm + m]);
+      double fo = -heff + a.c6 * c[l] + a.lambda * p2 * c[l];
+      if (l == 0) fo -= a.H;
+      out.c[l][own] = c[l] - a.dtg * fo + a.sq * xi[l];
+    }
   }
 }
 
 // ----------------------------------------------------------------------------
 // Fused ideal step (IdealPV2::step_no_reject, Stepper.cxx:68-176).
-// A CTA owns a TX x TY column of sites and marches up a z-chunk.  For every
-// plane it rotates phi by the half step (phi') for its sites and a one-site
-// ring around them into shared memory (3 rotating plane buffers), then for the
-// plane below: advects the charges with the 7-point stencil on phi', applies
-// the second half rotation with the updated charges and writes the site.
-// Reads each site once (80 B), writes it once (80 B) to the other buffer.
+// A CTA owns a TX x TY column of sites and marches up a z-chunk.  At plane p
+// it rotates phi by the half step (phi') for its sites and a one-site ring
+// into shared memory (3 rotating plane buffers); for plane p-1 it advects the
+// charges with the 7-point stencil on phi', applies the second half rotation
+// with the updated charges and writes the site to `out`.  The 10 components
+// of plane p+1 arrive by cp.async while plane p computes.  Each site is read
+// once (80 B) and written once (80 B).
+template <int TX, int TY>
+struct IdealTile {
+  static constexpr int SX = TX + 2, SY = TY + 2, SP = SX * SY;
+  static constexpr int NHALO = 2 * SX + 2 * TY;
+  static constexpr size_t SMEM = (size_t)(2 * 10 * SP + 3 * 4 * SP) * sizeof(double);
+};
+
 template <int TX, int TY>
 __global__ void __launch_bounds__(TX *TY, 2) ideal_kernel(Fields in, Fields out, Geo g, int zchunk, IdealArgs a) {
-  constexpr int SX = TX + 2, SY = TY + 2, SP = SX * SY;
-  constexpr int NHALO = 2 * SX + 2 * TY;
+  using T = IdealTile<TX, TY>;
+  constexpr int SX = T::SX, SY = T::SY, SP = T::SP, NHALO = T::NHALO;
   static_assert(NHALO <= TX * TY, "halo ring larger than the CTA");
-  __shared__ double sp[3][4][SP];
+  extern __shared__ double smem[];
+  double *raw = smem;               // [2 stages][10][SP]
+  double *phs = raw + 2 * 10 * SP;  // [3][4][SP]
   const int N = g.N;
   const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
   const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
   const int z0 = blockIdx.z * zchunk;
   const int z1 = min(z0 + zchunk, N);
+  const int nit = (z1 - z0) + 2;
   const bool act = (x0 + tx < N) && (y0 + ty < N);
   const int xi = (x0 + tx) % N, yj = (y0 + ty) % N;
   const int sc = (ty + 1) * SX + tx + 1;
@@ -401,61 +795,61 @@ __global__ void __launch_bounds__(TX *TY, 2) ideal_kernel(Fields in, Fields out,
     else if (h < 2 * SX + TY) { hx = 0; hy = 1 + (h - 2 * SX); }
     else { hx = SX - 1; hy = 1 + (h - 2 * SX - TY); }
     hs = hy * SX + hx;
-    hxg = ((x0 - 1 + hx) % N + N) % N;
-    hyg = ((y0 - 1 + hy) % N + N) % N;
+    hxg = wrapn(x0 - 1 + hx, N);
+    hyg = wrapn(y0 - 1 + hy, N);
   }
 
-  auto load = [&](int ii, int jj, int kk, double phi[4], double q[6]) {
-    const long long o = rb_off(g, ii, jj, kk);
+  auto issue = [&](int plane, int stage, bool halo) {
+    const long long o = rb_off(g, xi, yj, plane);
 #pragma unroll
-    for (int l = 0; l < 4; ++l) phi[l] = in.c[l][o];
+    for (int c = 0; c < 10; ++c) cp_async8(&raw[(stage * 10 + c) * SP + sc], in.c[c] + o);
+    if (halo && hs >= 0) {
+      const long long oh = rb_off(g, hxg, hyg, plane);
 #pragma unroll
-    for (int s = 0; s < 6; ++s) q[s] = in.c[4 + s][o];
+      for (int c = 0; c < 10; ++c) cp_async8(&raw[(stage * 10 + c) * SP + hs], in.c[c] + oh);
+    }
   };
 
-  double pm[4], pc[4], pn[4], qc[6], qn[6];
-  {
-    const int km = z0 == 0 ? N - 1 : z0 - 1;
-    double q[6];
-    load(xi, yj, km, pm, q);
-    rotate_site(pm, q, a.dto2chi);
-  }
-  load(xi, yj, z0, pc, qc);
-  rotate_site(pc, qc, a.dto2chi);
-#pragma unroll
-  for (int l = 0; l < 4; ++l) sp[0][l][sc] = pc[l];
-  if (hs >= 0) {
-    double ph[4], qh[6];
-    load(hxg, hyg, z0, ph, qh);
-    rotate_site(ph, qh, a.dto2chi);
-#pragma unroll
-    for (int l = 0; l < 4; ++l) sp[0][l][hs] = ph[l];
-  }
+  issue(wrapn(z0 - 1, N), 0, false);
+  cp_async_commit();
 
-  int bc = 0;
-  for (int kc = z0; kc < z1; ++kc) {
-    const int kn = (kc + 1 == N) ? 0 : kc + 1;
-    const int bn = (bc == 2) ? 0 : bc + 1;
-    load(xi, yj, kn, pn, qn);
+  double pm[4], pc[4], pn[4], qc[6], qn[6];
+  for (int it = 0; it < nit; ++it) {
+    const int p = wrapn(z0 - 1 + it, N);
+    cp_async_wait_all();
+    __syncthreads();
+    if (it + 1 < nit) issue(wrapn(p + 1, N), (it + 1) & 1, true);
+    cp_async_commit();
+
+    const double *rw = raw + (it & 1) * 10 * SP;
+    double *ph = phs + (it % 3) * 4 * SP;
+#pragma unroll
+    for (int l = 0; l < 4; ++l) pn[l] = rw[l * SP + sc];
+#pragma unroll
+    for (int s = 0; s < 6; ++s) qn[s] = rw[(4 + s) * SP + sc];
     rotate_site(pn, qn, a.dto2chi);
 #pragma unroll
-    for (int l = 0; l < 4; ++l) sp[bn][l][sc] = pn[l];
-    if (hs >= 0) {
-      double ph[4], qh[6];
-      load(hxg, hyg, kn, ph, qh);
-      rotate_site(ph, qh, a.dto2chi);
+    for (int l = 0; l < 4; ++l) ph[l * SP + sc] = pn[l];
+    if (hs >= 0 && it >= 1) {
+      double phh[4], qh[6];
 #pragma unroll
-      for (int l = 0; l < 4; ++l) sp[bn][l][hs] = ph[l];
+      for (int l = 0; l < 4; ++l) phh[l] = rw[l * SP + hs];
+#pragma unroll
+      for (int s = 0; s < 6; ++s) qh[s] = rw[(4 + s) * SP + hs];
+      rotate_site(phh, qh, a.dto2chi);
+#pragma unroll
+      for (int l = 0; l < 4; ++l) ph[l * SP + hs] = phh[l];
     }
-    __syncthreads();
-    if (act) {
+
+    if (it >= 2 && act) {
+      const double *pp = phs + ((it + 2) % 3) * 4 * SP;  // phi' of plane p-1 (written last iteration)
       double xp[4], xm[4], yp[4], ym[4];
 #pragma unroll
       for (int l = 0; l < 4; ++l) {
-        xp[l] = sp[bc][l][sc + 1];
-        xm[l] = sp[bc][l][sc - 1];
-        yp[l] = sp[bc][l][sc + SX];
-        ym[l] = sp[bc][l][sc - SX];
+        xp[l] = pp[l * SP + sc + 1];
+        xm[l] = pp[l * SP + sc - 1];
+        yp[l] = pp[l * SP + sc + SX];
+        ym[l] = pp[l * SP + sc - SX];
       }
       const double *c = pc, *zp = pn, *zm = pm;
       // axial charges (Stepper.cxx:112-133)
@@ -475,10 +869,10 @@ __global__ void __launch_bounds__(TX *TY, 2) ideal_kernel(Fields in, Fields out,
         const double bz = zp[s2] * c[s1] - c[s2] * zm[s1] - zp[s1] * c[s2] + c[s1] * zm[s2];
         qc[3 + s] += a.dt * (bx * a.a2 + by * a.a2 + bz * a.a2);
       }
-      // second half rotation on a copy: pc (phi') is still the z-1 neighbour of the next plane
+      // second half rotation on a copy: pc (phi') stays the z-1 neighbour of the next plane
       double pf[4] = {pc[0], pc[1], pc[2], pc[3]};
       rotate_site(pf, qc, a.dto2chi);
-      const long long o = rb_off(g, xi, yj, kc);
+      const long long o = rb_off(g, xi, yj, wrapn(p - 1, N));
 #pragma unroll
       for (int l = 0; l < 4; ++l) out.c[l][o] = pf[l];
 #pragma unroll
@@ -491,7 +885,6 @@ __global__ void __launch_bounds__(TX *TY, 2) ideal_kernel(Fields in, Fields out,
     }
 #pragma unroll
     for (int s = 0; s < 6; ++s) qc[s] = qn[s];
-    bc = bn;
   }
 }
 
@@ -849,50 +1242,164 @@ cudaError_t launch_init_charges(Fields f, int N, uint64_t sk, double sqrtchi, do
   return cudaGetLastError();
 }
 
+template <typename K>
+static cudaError_t allow_smem(K kernel, size_t bytes) {
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
 cudaError_t launch_hb_pass(Fields f, int N, int parity, const HbArgs &a, cudaStream_t st) {
   const Geo g = make_geo(N);
-  const unsigned nb = nblocks(g.V2, kThreads);
-  const bool inj = a.prop != nullptr;
-  const bool mon = a.mon != nullptr;
+  dim3 grid((g.H + 127) / 128, N, N);
+  const bool inj = a.prop != nullptr, mon = a.mon != nullptr;
   if (inj) {
-    if (mon) hb_pass_kernel<true, true><<<nb, kThreads, 0, st>>>(f, g, parity, a);
-    else hb_pass_kernel<true, false><<<nb, kThreads, 0, st>>>(f, g, parity, a);
+    if (mon) hb_pass_kernel<true, true><<<grid, 128, 0, st>>>(f, g, parity, a);
+    else hb_pass_kernel<true, false><<<grid, 128, 0, st>>>(f, g, parity, a);
   } else {
-    if (mon) hb_pass_kernel<false, true><<<nb, kThreads, 0, st>>>(f, g, parity, a);
-    else hb_pass_kernel<false, false><<<nb, kThreads, 0, st>>>(f, g, parity, a);
+    if (mon) hb_pass_kernel<false, true><<<grid, 128, 0, st>>>(f, g, parity, a);
+    else hb_pass_kernel<false, false><<<grid, 128, 0, st>>>(f, g, parity, a);
+  }
+  return cudaGetLastError();
+}
+
+static int hb_zchunk(int N) {
+  const int H = N / 2;
+  const long long bxy = (long long)((H + HB_TM - 1) / HB_TM) * ((N + HB_TY - 1) / HB_TY);
+  long long z = (long long)N * bxy / 1184;  // aim at >= 4 CTAs per SM slot
+  if (z > 32) z = 32;
+  if (z < 4) z = 4;
+  if (z > N) z = N;
+  return (int)z;
+}
+
+cudaError_t launch_hb_sweep(Fields in, Fields out, int N, const HbArgs &a, cudaStream_t st) {
+  const Geo g = make_geo(N);
+  const int zc = hb_zchunk(N);
+  dim3 grid((g.H + HB_TM - 1) / HB_TM, (N + HB_TY - 1) / HB_TY, (N + zc - 1) / zc);
+  const bool inj = a.prop != nullptr, mon = a.mon != nullptr;
+  cudaError_t e;
+  if (inj) {
+    if (mon) {
+      if ((e = allow_smem(hb_sweep_kernel<true, true>, HB_SMEM)) != cudaSuccess) return e;
+      hb_sweep_kernel<true, true><<<grid, HB_TM * HB_TY, HB_SMEM, st>>>(in, out, g, zc, a);
+    } else {
+      if ((e = allow_smem(hb_sweep_kernel<true, false>, HB_SMEM)) != cudaSuccess) return e;
+      hb_sweep_kernel<true, false><<<grid, HB_TM * HB_TY, HB_SMEM, st>>>(in, out, g, zc, a);
+    }
+  } else {
+    if (mon) {
+      if ((e = allow_smem(hb_sweep_kernel<false, true>, HB_SMEM)) != cudaSuccess) return e;
+      hb_sweep_kernel<false, true><<<grid, HB_TM * HB_TY, HB_SMEM, st>>>(in, out, g, zc, a);
+    } else {
+      if ((e = allow_smem(hb_sweep_kernel<false, false>, HB_SMEM)) != cudaSuccess) return e;
+      hb_sweep_kernel<false, false><<<grid, HB_TM * HB_TY, HB_SMEM, st>>>(in, out, g, zc, a);
+    }
   }
   return cudaGetLastError();
 }
 
 cudaError_t launch_charge_pass(Fields f, int N, int dir, int eoA, const ChargeArgs &a, cudaStream_t st) {
   const Geo g = make_geo(N);
-  const unsigned nb = nblocks(g.V2, kThreads);
+  dim3 grid((g.H + 127) / 128, N, N);
   const bool inj = a.q != nullptr;
   const bool mon = a.mon != nullptr;
   if (inj) {
-    if (mon) charge_pass_kernel<true, true><<<nb, kThreads, 0, st>>>(f, g, dir, eoA, a);
-    else charge_pass_kernel<true, false><<<nb, kThreads, 0, st>>>(f, g, dir, eoA, a);
+    if (mon) charge_pass_kernel<true, true><<<grid, 128, 0, st>>>(f, g, dir, eoA, a);
+    else charge_pass_kernel<true, false><<<grid, 128, 0, st>>>(f, g, dir, eoA, a);
   } else {
-    if (mon) charge_pass_kernel<false, true><<<nb, kThreads, 0, st>>>(f, g, dir, eoA, a);
-    else charge_pass_kernel<false, false><<<nb, kThreads, 0, st>>>(f, g, dir, eoA, a);
+    if (mon) charge_pass_kernel<false, true><<<grid, 128, 0, st>>>(f, g, dir, eoA, a);
+    else charge_pass_kernel<false, false><<<grid, 128, 0, st>>>(f, g, dir, eoA, a);
   }
+  return cudaGetLastError();
+}
+
+static int charge_seglen(int N) { return N >= 64 ? 32 : N; }
+
+cudaError_t launch_charge_dir(Fields in, Fields out, int N, int dir, const ChargeDirPair &p, cudaStream_t st,
+                              bool *swapped) {
+  const Geo g = make_geo(N);
+  ChargeDirArgs a;
+  a.rms = p.rms;
+  a.inv2chi = p.inv2chi;
+  for (int i = 0; i < 2; ++i) {
+    a.sk[i] = p.sk[i];
+    a.pass[i] = p.pass[i];
+    a.eo[i] = p.eo[i];
+  }
+  a.q = p.q;
+  a.acc = p.acc;
+  a.flags = p.flags;
+  a.mon = p.mon;
+  const bool inj = a.q != nullptr, mon = a.mon != nullptr;
+  if (dir == 0 && g.H > 256) {
+    // rows longer than one 256-thread CTA: the two faces as separate launches
+    *swapped = false;
+    for (int i = 0; i < 2; ++i) {
+      ChargeArgs c{};
+      c.rms = p.rms;
+      c.inv2chi = p.inv2chi;
+      c.sk = p.sk[i];
+      c.pass = p.pass[i];
+      c.q = p.q;
+      c.acc = p.acc;
+      c.flags = p.flags;
+      c.mon = p.mon;
+      cudaError_t e = launch_charge_pass(in, N, 0, p.eo[i], c, st);
+      if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+  }
+  if (dir == 0) {
+    *swapped = false;
+    const int H = g.H;
+    const int by = H >= 256 ? 1 : 256 / H;
+    const long long rows = (long long)N * N;
+    dim3 block(H, by), grid((unsigned)((rows + by - 1) / by));
+    const size_t sm = (size_t)6 * by * H * sizeof(double);
+    if (inj) {
+      if (mon) charge_x_kernel<true, true><<<grid, block, sm, st>>>(in, g, a);
+      else charge_x_kernel<true, false><<<grid, block, sm, st>>>(in, g, a);
+    } else {
+      if (mon) charge_x_kernel<false, true><<<grid, block, sm, st>>>(in, g, a);
+      else charge_x_kernel<false, false><<<grid, block, sm, st>>>(in, g, a);
+    }
+    return cudaGetLastError();
+  }
+  *swapped = true;
+  const int sl = charge_seglen(N);
+  dim3 grid((g.H + 127) / 128, N, (N + sl - 1) / sl);
+#define LGV_LINE(D, I, M) charge_line_kernel<D, I, M><<<grid, 128, 0, st>>>(in, out, g, a, sl)
+  if (dir == 1) {
+    if (inj) { if (mon) LGV_LINE(1, true, true); else LGV_LINE(1, true, false); }
+    else { if (mon) LGV_LINE(1, false, true); else LGV_LINE(1, false, false); }
+  } else {
+    if (inj) { if (mon) LGV_LINE(2, true, true); else LGV_LINE(2, true, false); }
+    else { if (mon) LGV_LINE(2, false, true); else LGV_LINE(2, false, false); }
+  }
+#undef LGV_LINE
   return cudaGetLastError();
 }
 
 cudaError_t launch_em(Fields in, Fields out, int N, const EmArgs &a, cudaStream_t st) {
   const Geo g = make_geo(N);
-  const unsigned nb = nblocks(2 * g.V2, kThreads);
-  if (a.xi) em_kernel<true><<<nb, kThreads, 0, st>>>(in, out, g, a);
-  else em_kernel<false><<<nb, kThreads, 0, st>>>(in, out, g, a);
+  dim3 grid((g.H + 127) / 128, N, N);
+  if (a.xi) em_kernel<true><<<grid, 128, 0, st>>>(in, out, g, a);
+  else em_kernel<false><<<grid, 128, 0, st>>>(in, out, g, a);
   return cudaGetLastError();
 }
 
 cudaError_t launch_ideal(Fields in, Fields out, int N, const IdealArgs &a, cudaStream_t st) {
   const Geo g = make_geo(N);
   constexpr int TX = 32, TY = 8;
-  const int zchunk = N >= 128 ? 32 : (N >= 32 ? 16 : N);
-  dim3 grid((N + TX - 1) / TX, (N + TY - 1) / TY, (N + zchunk - 1) / zchunk);
-  ideal_kernel<TX, TY><<<grid, TX * TY, 0, st>>>(in, out, g, zchunk, a);
+  using T = IdealTile<TX, TY>;
+  const long long bxy = (long long)((N + TX - 1) / TX) * ((N + TY - 1) / TY);
+  long long zc = (long long)N * bxy / 1184;
+  if (zc > 32) zc = 32;
+  if (zc < 4) zc = 4;
+  if (zc > N) zc = N;
+  dim3 grid((N + TX - 1) / TX, (N + TY - 1) / TY, (unsigned)((N + zc - 1) / zc));
+  cudaError_t e = allow_smem(ideal_kernel<TX, TY>, T::SMEM);
+  if (e != cudaSuccess) return e;
+  ideal_kernel<TX, TY><<<grid, TX * TY, T::SMEM, st>>>(in, out, g, (int)zc, a);
   return cudaGetLastError();
 }
 

@@ -287,3 +287,71 @@ def test_injected_noise_required(lgv):
     g.mode(INJECTED)
     with pytest.raises(L.LgvError):
         g.step(HB, 0.01)
+
+
+@pytest.mark.parametrize("N,mode", [(4, COUNTER), (8, INJECTED), (16, COUNTER), (34, COUNTER), (66, INJECTED)])
+def test_phi_heatbath_fused_sweep_variant(lgv, oracle_mod, N, mode, monkeypatch):
+    """The z-marching single-launch sweep (LGV_HB_FUSED=1) gives the oracle's
+    result too: the same decisions from the same streams."""
+    monkeypatch.setenv("LGV_HB_FUSED", "1")
+    g, o = pair(lgv, oracle_mod, N, oracle_mod.INJECTED if mode else oracle_mod.COUNTER)
+    monkeypatch.delenv("LGV_HB_FUSED")
+    u = rand_state(N, 111 + N)
+    g.set_state(u)
+    o.set_state(u)
+    g.flags(True)
+    o.debug_flags(True)
+    if mode == INJECTED:
+        g.mode(INJECTED)
+        prop, acc = hb_noise(N, 112)
+        g.inject_hb(prop, acc)
+        o.inject_hb(prop, acc)
+        g.step(HB, 0.02)
+        o.step(HB, 0.02)
+    else:
+        g.step(HB, 0.02, nsteps=3)
+        o.step(HB, 0.02, nsteps=3)
+    assert compare_flags(g.get_flags(), o.get_flags(), N ** 3) == 0
+    assert_state_close(g.get_state(), o.get_state(), what="fused HB sweep")
+
+
+@pytest.mark.parametrize("N,seed,fused", [(64, 15, True), (66, 16, True), (8, 17, True), (66, 18, False)])
+def test_charge_heatbath_injected_segments_and_fused(lgv, oracle_mod, N, seed, fused, monkeypatch):
+    """LGV_CHARGE_FUSED=1 runs both faces of a direction per launch: x rows
+    per CTA, y and z streamed in 32-site segments with two-site halos for
+    N >= 64 (66 leaves a ragged last segment).  Both it and the default
+    single-face launches reproduce the oracle decision for decision."""
+    if fused:
+        monkeypatch.setenv("LGV_CHARGE_FUSED", "1")
+    g, o = pair(lgv, oracle_mod, N, oracle_mod.INJECTED)
+    monkeypatch.delenv("LGV_CHARGE_FUSED", raising=False)
+    u = rand_state(N, seed)
+    g.set_state(u)
+    o.set_state(u)
+    g.mode(INJECTED)
+    g.flags(True)
+    o.debug_flags(True)
+    g.monitors(True)
+    order, q, acc = charge_noise(N, seed)
+    g.inject_charge(order, q, acc)
+    o.inject_charge(order, q, acc)
+    g.step(CHARGE, 0.04)
+    o.step(CHARGE, 0.04)
+    assert compare_flags(g.get_flags(), o.get_flags(), 36 * N ** 3) == 0
+    assert_state_close(g.get_state(), o.get_state(), what="charge HB segments")
+    gm, om = g.monitors()[2], o.monitor(2)
+    for k in ("down_counts", "up_counts", "up_yes", "up_no"):
+        assert gm[k] == om[k], k
+
+
+@pytest.mark.parametrize("N", [64, 70])
+def test_charge_heatbath_counter_segments(lgv, oracle_mod, N, monkeypatch):
+    monkeypatch.setenv("LGV_CHARGE_FUSED", "1")
+    g, o = pair(lgv, oracle_mod, N, oracle_mod.COUNTER)
+    monkeypatch.delenv("LGV_CHARGE_FUSED")
+    u = rand_state(N, 19)
+    g.set_state(u)
+    o.set_state(u)
+    g.step(CHARGE, 0.2, nsteps=2)
+    o.step(CHARGE, 0.2, nsteps=2)
+    assert_state_close(g.get_state(), o.get_state(), what="charge HB counter segments")
