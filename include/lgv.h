@@ -189,7 +189,9 @@ int lgv_enable_monitors(lgv_handle *h, int enable);
 int lgv_get_monitor(lgv_handle *h, int which, lgv_monitor *out);
 
 /* Stream control: all work of the handle is issued on this cudaStream_t
- * (NULL = the legacy default stream). */
+ * (NULL = the legacy default stream).  A new handle uses a non-blocking stream
+ * of its own.  Work already queued on the previous stream is ordered before
+ * any work issued on the new one. */
 int lgv_set_stream(lgv_handle *h, void *cuda_stream);
 int lgv_synchronize(lgv_handle *h);
 

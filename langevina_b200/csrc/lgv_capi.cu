@@ -659,7 +659,17 @@ int lgv_get_monitor(lgv_handle *h, int which, lgv_monitor *out) {
 
 int lgv_set_stream(lgv_handle *h, void *s) {
   if (!h) return fail(LGV_ERR_INVALID, "handle is NULL");
-  h->stream = s ? (cudaStream_t)s : h->own_stream;
+  // NULL selects the legacy default stream, as documented in lgv.h
+  cudaStream_t next = s ? (cudaStream_t)s : (cudaStream_t)0;
+  if (next == h->stream) return LGV_OK;
+  // work already queued on the old stream must finish before the new
+  // stream touches the lattice
+  DeviceGuard g(h->device);
+  cudaEvent_t ev = pool_event(h);
+  LGV_CK(cudaEventRecord(ev, h->stream));
+  LGV_CK(cudaStreamWaitEvent(next, ev, 0));
+  h->ev_pool.push_back(ev);
+  h->stream = next;
   return LGV_OK;
 }
 

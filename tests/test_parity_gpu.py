@@ -355,3 +355,24 @@ def test_charge_heatbath_counter_segments(lgv, oracle_mod, N, monkeypatch):
     g.step(CHARGE, 0.2, nsteps=2)
     o.step(CHARGE, 0.2, nsteps=2)
     assert_state_close(g.get_state(), o.get_state(), what="charge HB counter segments")
+
+
+def test_stream_switch_keeps_order(lgv):
+    """Work queued on the handle's stream finishes before a newly set stream
+    touches the lattice (lgv_set_stream orders the two streams)."""
+    import ctypes as C
+
+    import torch
+
+    N = 48
+    u = rand_state(N, 131)
+    a = GpuLattice(lgv, N, **COEF)
+    a.set_state(u)
+    a.step(PV2, 0.04, nsteps=30, inner=2, outer=3)
+    want = a.get_state()
+    b = GpuLattice(lgv, N, **COEF)
+    b.set_state(u)
+    b.step(PV2, 0.04, nsteps=30, inner=2, outer=3)  # queued on b's own stream, not synchronized
+    s = torch.cuda.Stream()
+    b.L.check(b.lib.lgv_set_stream(b.h, C.c_void_p(s.cuda_stream)), "set_stream")
+    assert np.array_equal(b.get_state(), want)
