@@ -19,8 +19,27 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
+DRIVER = os.path.join(HERE, "superpions")
+CXX = os.environ.get("CXX", "g++")
+
+
 def sources():
     return sorted(glob.glob(os.path.join(HERE, "csrc", "*.cu")))
+
+
+def build_driver():
+    """The C++ run driver (csrc/superpions.cpp) over include/langevina.hpp, linked to liblgv.so."""
+    src = os.path.join(HERE, "csrc", "superpions.cpp")
+    deps = [src, LIB, os.path.join(REPO, "include", "langevina.hpp"), os.path.join(REPO, "include", "lgv.h")]
+    if os.path.exists(DRIVER) and all(os.path.getmtime(d) <= os.path.getmtime(DRIVER) for d in deps):
+        return DRIVER
+    cmd = [CXX, "-O2", "-std=c++17", "-Wall", "-I", os.path.join(REPO, "include"), src, "-o", DRIVER,
+           "-L", HERE, "-llgv", "-Wl,-rpath,$ORIGIN"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("g++ failed building the superpions driver")
+    return DRIVER
 
 
 def headers():
@@ -37,6 +56,7 @@ def up_to_date():
 
 def build(verbose=False, force=False):
     if not force and up_to_date():
+        build_driver()
         return LIB
     cmd = [NVCC, "-O3", "-std=c++17", *ARCH, "-lineinfo", "--shared", "-Xcompiler", "-fPIC",
            "-I", os.path.join(REPO, "include"), "-o", LIB, *sources()]
@@ -48,6 +68,7 @@ def build(verbose=False, force=False):
         raise RuntimeError("nvcc failed building liblgv.so")
     if verbose:
         sys.stderr.write(r.stderr)
+    build_driver()
     return LIB
 
 
