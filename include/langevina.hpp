@@ -630,7 +630,7 @@ class Measurer {
   void measure() {
     lgv_measurement m{};
     m.OAverage = OAverage.data();
-    auto *W = std::array<nvector2<double> *, 3>{&wallX, &wallY, &wallZ}.data();
+    nvector2<double> *W[3] = {&wallX, &wallY, &wallZ};
     nvector2<double> *P[3] = {&wallXPhase, &wallYPhase, &wallZPhase};
     nvector2<std::complex<double>> *K[3] = {&wallX_k, &wallY_k, &wallZ_k};
     nvector2<std::complex<double>> *R[3] = {&wallX_k_rotated, &wallY_k_rotated, &wallZ_k_rotated};
