@@ -50,7 +50,7 @@ MEASURE_EVERY = 10
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--N", type=int, default=256)
@@ -58,6 +58,7 @@ def parse():
     ap.add_argument("--seed", type=int, default=122335456)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true")
     return ap.parse_args()
 
 
@@ -161,6 +162,88 @@ def run_reference(a):
     }
     print(json.dumps(line))
     return 0
+
+
+ENSEMBLE = [(32, 256), (48, 64), (64, 16)]  # (N, replicas)
+ENS_H = (0.003, 0.006, 0.012)
+
+
+def run_ensemble(steps=20, plain_steps=2):
+    """Batched ensemble (one launch per sub-step over all replicas, autotuned,
+    two-step CUDA graphs) vs looping the single-lattice path one replica per
+    launch.  Returns replica-steps/s of both."""
+    import ctypes as C
+
+    import torch
+    from langevina_b200 import _lib as L
+
+    lib = L.load()
+    specs = []
+    for N, n in ENSEMBLE:
+        for _ in range(n):
+            specs.append((N, 1000 + len(specs), ENS_H[len(specs) % 3]))
+    R = len(specs)
+    sites = sum(N ** 3 for N, _, _ in specs)
+    arr = (L.lgv_params * R)()
+    for i, (N, seed, H) in enumerate(specs):
+        arr[i] = L.make_params(N, seed=seed, **dict(COEF, H=H))
+    e = C.c_void_p()
+    L.check(lib.lgv_ensemble_create(R, arr, C.byref(e)), "ensemble_create")
+    stream = torch.cuda.Stream()
+    L.check(lib.lgv_ensemble_set_stream(e, C.c_void_p(stream.cuda_stream)), "ens stream")
+    L.check(lib.lgv_ensemble_initialize(e, L.INIT_PHI_GAUSSIAN, 0.1), "init")
+    L.check(lib.lgv_ensemble_initialize(e, L.INIT_CHARGES_GAUSSIAN, 0.0), "init")
+    choice = (C.c_int * 3)()
+    tms = C.c_double()
+    L.check(lib.lgv_ensemble_autotune(e, L.PV2HBSPLIT, 2, 3, DT, 4, choice, C.byref(tms)), "autotune")
+    L.check(lib.lgv_ensemble_step(e, L.PV2HBSPLIT, 2, 3, DT, 0.0, 4), "warm")
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    L.check(lib.lgv_ensemble_step(e, L.PV2HBSPLIT, 2, 3, DT, 0.0, steps), "ens step")
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    lib.lgv_ensemble_destroy(e)
+
+    plain = {}
+    for mode in ("one_stream", "own_streams"):
+        hs = []
+        s1 = torch.cuda.Stream()
+        for N, seed, H in specs:
+            p = L.make_params(N, seed=seed, **dict(COEF, H=H))
+            h = C.c_void_p()
+            L.check(lib.lgv_create(C.byref(p), C.byref(h)), "create")
+            if mode == "one_stream":
+                L.check(lib.lgv_set_stream(h, C.c_void_p(s1.cuda_stream)), "stream")
+            L.check(lib.lgv_initialize(h, L.INIT_PHI_GAUSSIAN, 0.1), "init")
+            L.check(lib.lgv_initialize(h, L.INIT_CHARGES_GAUSSIAN, 0.0), "init")
+            hs.append(h)
+        for h in hs:
+            L.check(lib.lgv_step(h, L.PV2HBSPLIT, 2, 3, DT, 0.0, 1), "warm")
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(plain_steps):
+            for h in hs:
+                L.check(lib.lgv_step(h, L.PV2HBSPLIT, 2, 3, DT, 0.0, 1), "step")
+        torch.cuda.synchronize()
+        plain[mode] = (time.perf_counter() - t0) / plain_steps * 1e3
+        for h in hs:
+            lib.lgv_destroy(h)
+    best_plain = min(plain.values())
+    return {
+        "workload": "PV2HBSplit23, 256 x 32^3 + 64 x 48^3 + 16 x 64^3 replicas, distinct seeds, "
+                    "H in (0.003, 0.006, 0.012) round robin, config-1 coefficients",
+        "replicas": R, "sites": sites,
+        "batched_ms_per_step": ms, "batched_replica_steps_per_s": R / (ms / 1e3),
+        "batched_site_updates_per_s": sites / (ms / 1e3),
+        "autotune_choice": {"tile": ["32x8", "16x16"][choice[0]], "zchunk": choice[1],
+                            "packing": ["given", "largest_first", "interleaved"][choice[2]]},
+        "plain_ms_per_step": plain, "plain_replica_steps_per_s": R / (best_plain / 1e3),
+        "speedup_vs_plain": best_plain / ms,
+        "timing": "batched: CUDA events over graph replays; plain: host wall clock around a loop of lgv_step, "
+                  "one replica per call (one shared stream / each handle on its own stream)",
+    }
 
 
 def run_ours(a):
@@ -306,6 +389,9 @@ def run_ours(a):
 
     lgv_destroy = lib.lgv_destroy
     lgv_destroy(h)
+    ensemble = None
+    if world == 1 and not a.no_ensemble:
+        ensemble = run_ensemble()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -324,6 +410,7 @@ def run_ours(a):
         "kernels": kernels,
         "cpu_baseline": cpu,
         "e2e": e2e,
+        "ensemble": ensemble,
         "gpu_launches": launches,
         "clocks": ck,
     }

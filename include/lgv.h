@@ -218,6 +218,47 @@ int lgv_timing_read(lgv_handle *h, int kclass, double *total_ms, int64_t *launch
 int lgv_debug_flags(lgv_handle *h, int enable);
 int lgv_get_flags(lgv_handle *h, uint8_t *host_out);
 
+/* ---------------------------------------------------------------------------
+ * Batched ensembles.  Replaces running an ensemble as separate processes or
+ * events, one lattice at a time (eventmode loop SuperPions.cxx:228-235, SLURM
+ * job arrays grunner.py:153-241): nrep independent replicas, each with its own
+ * lgv_params (any mix of N, seed and coefficients), advance together -- one
+ * launch per sub-step over all replicas, two steps per replayed CUDA graph.
+ * Replica r evolves exactly as an lgv handle created with params[r] and
+ * stepped with the same counter.  The packing order is the order in which
+ * replicas' blocks fill the grid. */
+typedef struct lgv_ensemble lgv_ensemble;
+#define LGV_PACK_GIVEN 0
+#define LGV_PACK_LARGEST_FIRST 1
+#define LGV_PACK_INTERLEAVED 2
+/* ideal-kernel tile shapes */
+#define LGV_TILE_32x8 0
+#define LGV_TILE_16x16 1
+int lgv_ensemble_create(int nrep, const lgv_params *params, lgv_ensemble **out);
+int lgv_ensemble_destroy(lgv_ensemble *e);
+int lgv_ensemble_size(lgv_ensemble *e, int *nrep);
+int lgv_ensemble_set_state(lgv_ensemble *e, int replica, const double *host_aos);
+int lgv_ensemble_get_state(lgv_ensemble *e, int replica, double *host_aos);
+/* as lgv_initialize, for every replica (one counter value for the ensemble) */
+int lgv_ensemble_initialize(lgv_ensemble *e, int kind, double scale);
+int lgv_ensemble_set_counter(lgv_ensemble *e, uint64_t counter);
+int lgv_ensemble_get_counter(lgv_ensemble *e, uint64_t *counter);
+/* as lgv_step, for every replica; asynchronous */
+int lgv_ensemble_step(lgv_ensemble *e, int evolver, int inner, int outer, double dt, double t, int nsteps);
+/* volume averages of the 11 OAverage observables, [nrep][11] */
+int lgv_ensemble_oaverage(lgv_ensemble *e, double *host_out);
+int lgv_ensemble_oaverage_device(lgv_ensemble *e, double *dev_out);
+/* explicit tuning: ideal tile (LGV_TILE_*), its z-chunk, packing (LGV_PACK_*) */
+int lgv_ensemble_tune(lgv_ensemble *e, int tile, int zchunk, int order);
+/* time every (tile, z-chunk in {8,16,32}, packing) candidate over `steps`
+ * steps on a copy of the state (state and counter restored), keep the
+ * fastest; choice[3] = (tile, zchunk, order), *ms_per_step its time */
+int lgv_ensemble_autotune(lgv_ensemble *e, int evolver, int inner, int outer, double dt, int steps, int *choice,
+                          double *ms_per_step);
+int lgv_ensemble_use_graphs(lgv_ensemble *e, int enable);
+int lgv_ensemble_set_stream(lgv_ensemble *e, void *cuda_stream);
+int lgv_ensemble_synchronize(lgv_ensemble *e);
+
 /* Allocation-free measurement.  No counterpart in the reference: it is the
  * measurement of lgv_measure_device() for callers that cannot allocate device
  * memory while they run -- a host whose GPU memory belongs to another

@@ -22,6 +22,8 @@ NOISE_COUNTER, NOISE_INJECTED = 0, 1
 INIT_ZERO, INIT_PHI_GAUSSIAN, INIT_CHARGES_GAUSSIAN = 0, 1, 2
 MONITOR_IDEAL, MONITOR_PHI_HB, MONITOR_CHARGE_HB = 0, 1, 2
 KCLASS_IDEAL, KCLASS_PHI_HB, KCLASS_CHARGE, KCLASS_EM, KCLASS_MEASURE = 0, 1, 2, 3, 4
+PACK_GIVEN, PACK_LARGEST_FIRST, PACK_INTERLEAVED = 0, 1, 2
+TILE_32x8, TILE_16x16 = 0, 1
 
 
 class lgv_params(C.Structure):
@@ -80,6 +82,23 @@ SIGNATURES = [
     ("lgv_debug_flags", C.c_int, [_H, C.c_int]),
     ("lgv_get_flags", C.c_int, [_H, C.c_void_p]),
     ("lgv_measure_aos_noalloc", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    ("lgv_ensemble_create", C.c_int, [C.c_int, C.c_void_p, C.POINTER(_H)]),
+    ("lgv_ensemble_destroy", C.c_int, [_H]),
+    ("lgv_ensemble_size", C.c_int, [_H, C.POINTER(C.c_int)]),
+    ("lgv_ensemble_set_state", C.c_int, [_H, C.c_int, C.c_void_p]),
+    ("lgv_ensemble_get_state", C.c_int, [_H, C.c_int, C.c_void_p]),
+    ("lgv_ensemble_initialize", C.c_int, [_H, C.c_int, C.c_double]),
+    ("lgv_ensemble_set_counter", C.c_int, [_H, C.c_uint64]),
+    ("lgv_ensemble_get_counter", C.c_int, [_H, C.POINTER(C.c_uint64)]),
+    ("lgv_ensemble_step", C.c_int, [_H, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int]),
+    ("lgv_ensemble_oaverage", C.c_int, [_H, C.c_void_p]),
+    ("lgv_ensemble_oaverage_device", C.c_int, [_H, C.c_void_p]),
+    ("lgv_ensemble_tune", C.c_int, [_H, C.c_int, C.c_int, C.c_int]),
+    ("lgv_ensemble_autotune", C.c_int, [_H, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, C.c_void_p,
+                                        C.POINTER(C.c_double)]),
+    ("lgv_ensemble_use_graphs", C.c_int, [_H, C.c_int]),
+    ("lgv_ensemble_set_stream", C.c_int, [_H, C.c_void_p]),
+    ("lgv_ensemble_synchronize", C.c_int, [_H]),
 ]
 
 _lib = None

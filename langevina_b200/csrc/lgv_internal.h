@@ -6,6 +6,7 @@
 
 #include <cstdint>
 
+#include "../../include/lgv.h"
 #include "lgv_device.cuh"
 
 namespace lgv {
@@ -66,6 +67,44 @@ struct IdealArgs {
   double a2;       // (1 / h)^2
   double H;
 };
+
+// ---------------------------------------------------------------------------
+// Batched ensembles: many independent lattices advanced by one launch per
+// sub-step.  Per-replica data lives in a device table; the sub-step counter
+// and the clock live in device memory so that captured CUDA graphs replay
+// with advancing noise.
+struct RepDesc {
+  double *base[2];     // the two lattice buffers; which is current is a launch argument
+  long long pstride;   // doubles from one component plane to the next (V + skew)
+  Geo g;
+  uint64_t key;  // make_key(seed)
+  double mass0, dmassdt, lambda, H, chi, gamma, diffusion, a2;
+  int nchunk;    // plane kernels: ceil(N * N/2 / 128) blocks per plane
+  int igx, igy, igz, izc;  // ideal kernel: tiles in x, y, z and the z-chunk
+};
+struct EnsDyn {
+  unsigned long long ctr;  // counter at the start of the current step
+  double t;                // clock at the start of the current step
+};
+
+
+// phase_phi / phase_q: which buffer holds the current phi / charges
+cudaError_t launch_batch_ideal(const RepDesc *d, const int *rep, const int *first, int nblocks, int tile,
+                               int phase_phi, int phase_q, double dt, cudaStream_t st);
+cudaError_t launch_batch_hb(const RepDesc *d, const EnsDyn *dyn, const int *rep, const int *first, int nblocks,
+                            int phase_phi, int parity, double dt, int ctr_off, cudaStream_t st);
+cudaError_t launch_batch_charge(const RepDesc *d, const EnsDyn *dyn, const int *rep, const int *first, int nblocks,
+                                int phase_q, int pass, double dt, int ctr_off_order, cudaStream_t st);
+cudaError_t launch_batch_em(const RepDesc *d, const EnsDyn *dyn, const int *rep, const int *first, int nblocks,
+                            int phase_phi, double dt, int ctr_off, cudaStream_t st);
+cudaError_t launch_ens_set(EnsDyn *dyn, unsigned long long ctr, double t, cudaStream_t st);
+cudaError_t launch_ens_advance(EnsDyn *dyn, unsigned long long dctr, double dt, cudaStream_t st);
+// volume averages (the 11 OAverage observables) of every replica: partial[nblocks][11], out[nrep][11]
+cudaError_t launch_batch_oavg(const RepDesc *d, const int *rep, const int *first, int nblocks, int phase_phi,
+                              int phase_q, double *partial, int nrep, double *out, cudaStream_t st);
+cudaError_t launch_batch_oavg_final(const RepDesc *d, const int *first, const int *count, int nrep,
+                                    const double *partial, double *out, cudaStream_t st);
+int ideal_tile_dims(int tile, int *tx, int *ty);
 
 // Launchers (lgv_kernels.cu).  All asynchronous on `st`; return cudaError_t.
 cudaError_t launch_aos_to_rb(const double *aos, Fields f, int N, cudaStream_t st);

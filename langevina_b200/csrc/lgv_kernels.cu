@@ -242,43 +242,47 @@ __device__ __forceinline__ void mon_count(MonLocal &m, const HbDecision &d) {
 // Phi heat bath, one checkerboard parity (EulerLangevinHB::step,
 // Stepper.cxx:325-381).  One thread per site of `parity`: element m of the
 // parity half-row (j, k); its six neighbours are elements of the other
-// parity's half-rows.  Grid: (m chunks, j, k), so no 64-bit index division.
+// parity's half-rows.
+template <bool INJECTED, bool MON>
+__device__ __forceinline__ void hb_site(const Fields &f, const Geo &g, int parity, const HbArgs &a, int m, int j,
+                                        int k, MonLocal &mon) {
+  const int H = g.H, N = g.N;
+  const int s = (parity + j + k) & 1;
+  int xm = m - 1 + s, xp = m + s;
+  if (xm < 0) xm += H;
+  if (xp == H) xp = 0;
+  const long long row = ((long long)k * N + j) * H;
+  const long long rjp = ((long long)k * N + wrap_inc(j, N)) * H;
+  const long long rjm = ((long long)k * N + wrap_dec(j, N)) * H;
+  const long long rkp = ((long long)wrap_inc(k, N) * N + j) * H;
+  const long long rkm = ((long long)wrap_dec(k, N) * N + j) * H;
+  const long long own = (long long)parity * g.V2 + row + m;
+  const long long ob = (long long)(parity ^ 1) * g.V2;
+  double po[4], heff[4];
+#pragma unroll
+  for (int l = 0; l < 4; ++l) {
+    const double *P = f.c[l];
+    heff[l] = (P[ob + row + xp] + P[ob + row + xm]) + (P[ob + rjp + m] + P[ob + rjm + m]) +
+              (P[ob + rkp + m] + P[ob + rkm + m]);
+    po[l] = P[own];
+  }
+  const long long nat = ((long long)k * N + j) * N + 2 * m + s;
+  HbDecision d;
+  hb_decide<INJECTED>(po, heff, a, nat, 2 * g.V2, d);
+  if (d.accept) {
+#pragma unroll
+    for (int l = 0; l < 4; ++l) f.c[l][own] = d.pn[l];
+  }
+  if (MON) mon_count(mon, d);
+  if (a.flags) a.flags[nat] = d.flag;
+}
+
+// Grid: (m chunks, j, k), so no 64-bit index division.
 template <bool INJECTED, bool MON>
 __global__ void __launch_bounds__(128) hb_pass_kernel(Fields f, Geo g, int parity, HbArgs a) {
   const int m = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y, k = blockIdx.z;
-  const int H = g.H, N = g.N;
   MonLocal mon;
-  if (m < H) {
-    const int s = (parity + j + k) & 1;
-    int xm = m - 1 + s, xp = m + s;
-    if (xm < 0) xm += H;
-    if (xp == H) xp = 0;
-    const long long row = ((long long)k * N + j) * H;
-    const long long rjp = ((long long)k * N + wrap_inc(j, N)) * H;
-    const long long rjm = ((long long)k * N + wrap_dec(j, N)) * H;
-    const long long rkp = ((long long)wrap_inc(k, N) * N + j) * H;
-    const long long rkm = ((long long)wrap_dec(k, N) * N + j) * H;
-    const long long own = (long long)parity * g.V2 + row + m;
-    const long long ob = (long long)(parity ^ 1) * g.V2;
-    double po[4], heff[4];
-#pragma unroll
-    for (int l = 0; l < 4; ++l) {
-      const double *P = f.c[l];
-      heff[l] = (P[ob + row + xp] + P[ob + row + xm]) + (P[ob + rjp + m] + P[ob + rjm + m]) +
-                (P[ob + rkp + m] + P[ob + rkm + m]);
-      po[l] = P[own];
-    }
-    const long long nat = ((long long)k * N + j) * N + 2 * m + s;
-    HbDecision d;
-    hb_decide<INJECTED>(po, heff, a, nat, 2 * g.V2, d);
-    if (d.accept) {
-#pragma unroll
-      for (int l = 0; l < 4; ++l) f.c[l][own] = d.pn[l];
-    }
-    if (MON) mon_count(mon, d);
-    if (a.flags) a.flags[nat] = d.flag;
-  }
+  if (m < g.H) hb_site<INJECTED, MON>(f, g, parity, a, m, blockIdx.y, blockIdx.z, mon);
   if (MON) mon_flush(mon, a.mon);
 }
 
@@ -429,70 +433,73 @@ __global__ void __launch_bounds__(HB_TM *HB_TY, 2) hb_sweep_kernel(Fields in, Fi
 // Charge heat bath, one face (direction `dir`, A-site parity eoA).  One thread
 // per link (A, B = A + e_dir); the links of a face are disjoint, so the update
 // is race free and conserves each charge exactly (Stepper.cxx:493-517).
+template <bool INJECTED, bool MON>
+__device__ __forceinline__ void charge_link_site(const Fields &f, const Geo &g, int dir, int eoA, const ChargeArgs &a,
+                                                 int m, int j, int k, MonLocal &mon) {
+  const int H = g.H, N = g.N;
+  const int s = (eoA + j + k) & 1;
+  const int i = 2 * m + s;
+  const long long offA = (long long)eoA * g.V2 + ((long long)k * N + j) * H + m;
+  long long offB;
+  const long long ob = (long long)(eoA ^ 1) * g.V2;
+  if (dir == 0) {
+    int mb = m + s;
+    if (mb == H) mb = 0;
+    offB = ob + ((long long)k * N + j) * H + mb;
+  } else if (dir == 1) {
+    offB = ob + ((long long)k * N + wrap_inc(j, N)) * H + m;
+  } else {
+    offB = ob + ((long long)wrap_inc(k, N) * N + j) * H + m;
+  }
+  const long long nat = ((long long)k * N + j) * N + i;
+  const long long V = 2 * g.V2;
+  Xoro rng;
+  if (!INJECTED) rng = stream_at(a.sk, (uint64_t)nat);
+#pragma unroll
+  for (int L = 0; L < 6; ++L) {
+    double *P = f.c[4 + L];
+    const double nA = P[offA], nB = P[offB];
+    const long long ii = (long long)(a.pass * 6 + L) * V + nat;
+    uint64_t ra = 0;
+    double v;
+    if (INJECTED) {
+      v = a.q[ii];
+    } else {
+      v = var1(rng.next());
+      ra = rng.next();
+    }
+    const double q = a.rms * v;
+    const double dA = nA - q, dB = nB + q;
+    const double dS = (dA * dA + dB * dB - nA * nA - nB * nB) * a.inv2chi;
+    bool accept;
+    uint8_t fl;
+    if (dS < 0) {
+      accept = true;
+      fl = 1;
+      if (MON) mon.down(dS);
+    } else {
+      const double r = INJECTED ? a.acc[ii] : u53(ra);
+      accept = r < exp(-dS);
+      fl = accept ? 2 : 0;
+      if (MON) {
+        if (accept) mon.up_yes(dS);
+        else mon.up_no();
+      }
+    }
+    if (accept) {
+      P[offA] = nA + (-q);
+      P[offB] = nB + q;
+    }
+    if (a.flags) a.flags[ii] = fl;
+  }
+}
+
 // Grid: (m chunks, j, k).
 template <bool INJECTED, bool MON>
 __global__ void __launch_bounds__(128) charge_pass_kernel(Fields f, Geo g, int dir, int eoA, ChargeArgs a) {
   const int m = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y, k = blockIdx.z;
-  const int H = g.H, N = g.N;
   MonLocal mon;
-  if (m < H) {
-    const int s = (eoA + j + k) & 1;
-    const int i = 2 * m + s;
-    const long long offA = (long long)eoA * g.V2 + ((long long)k * N + j) * H + m;
-    long long offB;
-    const long long ob = (long long)(eoA ^ 1) * g.V2;
-    if (dir == 0) {
-      int mb = m + s;
-      if (mb == H) mb = 0;
-      offB = ob + ((long long)k * N + j) * H + mb;
-    } else if (dir == 1) {
-      offB = ob + ((long long)k * N + wrap_inc(j, N)) * H + m;
-    } else {
-      offB = ob + ((long long)wrap_inc(k, N) * N + j) * H + m;
-    }
-    const long long nat = ((long long)k * N + j) * N + i;
-    const long long V = 2 * g.V2;
-    Xoro rng;
-    if (!INJECTED) rng = stream_at(a.sk, (uint64_t)nat);
-#pragma unroll
-    for (int L = 0; L < 6; ++L) {
-      double *P = f.c[4 + L];
-      const double nA = P[offA], nB = P[offB];
-      const long long ii = (long long)(a.pass * 6 + L) * V + nat;
-      uint64_t ra = 0;
-      double v;
-      if (INJECTED) {
-        v = a.q[ii];
-      } else {
-        v = var1(rng.next());
-        ra = rng.next();
-      }
-      const double q = a.rms * v;
-      const double dA = nA - q, dB = nB + q;
-      const double dS = (dA * dA + dB * dB - nA * nA - nB * nB) * a.inv2chi;
-      bool accept;
-      uint8_t fl;
-      if (dS < 0) {
-        accept = true;
-        fl = 1;
-        if (MON) mon.down(dS);
-      } else {
-        const double r = INJECTED ? a.acc[ii] : u53(ra);
-        accept = r < exp(-dS);
-        fl = accept ? 2 : 0;
-        if (MON) {
-          if (accept) mon.up_yes(dS);
-          else mon.up_no();
-        }
-      }
-      if (accept) {
-        P[offA] = nA + (-q);
-        P[offB] = nB + q;
-      }
-      if (a.flags) a.flags[ii] = fl;
-    }
-  }
+  if (m < g.H) charge_link_site<INJECTED, MON>(f, g, dir, eoA, a, m, blockIdx.y, blockIdx.z, mon);
   if (MON) mon_flush(mon, a.mon);
 }
 
@@ -706,11 +713,9 @@ __global__ void __launch_bounds__(128) charge_line_kernel(Fields in, Fields out,
 // Euler-Maruyama Model A step (Jacobi: reads `in`, writes phi of `out`).
 // One thread per element m of both parity half-rows of row (j, k).
 template <bool INJECTED>
-__global__ void __launch_bounds__(128) em_kernel(Fields in, Fields out, Geo g, EmArgs a) {
-  const int m = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y, k = blockIdx.z;
+__device__ __forceinline__ void em_pair(const Fields &in, const Fields &out, const Geo &g, const EmArgs &a, int m,
+                                        int j, int k) {
   const int H = g.H, N = g.N;
-  if (m >= H) return;
   const long long row = ((long long)k * N + j) * H;
   const long long rjp = ((long long)k * N + wrap_inc(j, N)) * H;
   const long long rjm = ((long long)k * N + wrap_dec(j, N)) * H;
@@ -752,6 +757,12 @@ __global__ void __launch_bounds__(128) em_kernel(Fields in, Fields out, Geo g, E
   }
 }
 
+template <bool INJECTED>
+__global__ void __launch_bounds__(128) em_kernel(Fields in, Fields out, Geo g, EmArgs a) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m < g.H) em_pair<INJECTED>(in, out, g, a, m, blockIdx.y, blockIdx.z);
+}
+
 // ----------------------------------------------------------------------------
 // Fused ideal step (IdealPV2::step_no_reject, Stepper.cxx:68-176).
 // A CTA owns a TX x TY column of sites and marches up a z-chunk.  At plane p
@@ -769,7 +780,8 @@ struct IdealTile {
 };
 
 template <int TX, int TY>
-__global__ void __launch_bounds__(TX *TY, 2) ideal_kernel(Fields in, Fields out, Geo g, int zchunk, IdealArgs a) {
+__device__ __forceinline__ void ideal_tile(const Fields &in, const Fields &out, const Geo &g, int zchunk,
+                                           const IdealArgs &a, int bx, int by, int bz) {
   using T = IdealTile<TX, TY>;
   constexpr int SX = T::SX, SY = T::SY, SP = T::SP, NHALO = T::NHALO;
   static_assert(NHALO <= TX * TY, "halo ring larger than the CTA");
@@ -778,8 +790,8 @@ __global__ void __launch_bounds__(TX *TY, 2) ideal_kernel(Fields in, Fields out,
   double *phs = raw + 2 * 10 * SP;  // [3][4][SP]
   const int N = g.N;
   const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
-  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
-  const int z0 = blockIdx.z * zchunk;
+  const int x0 = bx * TX, y0 = by * TY;
+  const int z0 = bz * zchunk;
   const int z1 = min(z0 + zchunk, N);
   const int nit = (z1 - z0) + 2;
   const bool act = (x0 + tx < N) && (y0 + ty < N);
@@ -886,6 +898,11 @@ __global__ void __launch_bounds__(TX *TY, 2) ideal_kernel(Fields in, Fields out,
 #pragma unroll
     for (int s = 0; s < 6; ++s) qc[s] = qn[s];
   }
+}
+
+template <int TX, int TY>
+__global__ void __launch_bounds__(TX *TY, 2) ideal_kernel(Fields in, Fields out, Geo g, int zchunk, IdealArgs a) {
+  ideal_tile<TX, TY>(in, out, g, zchunk, a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // ----------------------------------------------------------------------------
@@ -1204,6 +1221,178 @@ __global__ void meas_sum_k_aos_kernel(const double *__restrict__ aos, int N, dou
   for (int o = 0; o < kNObs; ++o) U[o * NN + (long long)j * N + i] = acc[o];
 }
 
+// ----------------------------------------------------------------------------
+// Batched kernels: one launch advances every replica of an ensemble.  The
+// flat grid is partitioned into per-replica block ranges (rep[b] is the
+// replica of block b, first[r] its first block; the order of the ranges is
+// the packing order chosen by the autotuner).  Each block rebuilds its
+// replica's arguments exactly as the single-lattice host code does (same
+// expressions, no FMA contraction), so a replica evolves bit for bit like a
+// lattice of its own; sub-step keys come from the device-resident counter.
+// the replica's planes: phi from buffer pphi, charges from buffer pq
+__device__ __forceinline__ Fields rep_fields(const RepDesc &r, int pphi, int pq) {
+  Fields f;
+#pragma unroll
+  for (int L = 0; L < 10; ++L) f.c[L] = r.base[L < 4 ? pphi : pq] + (long long)L * r.pstride;
+  return f;
+}
+
+__device__ __forceinline__ double rep_mass(const RepDesc &r, const EnsDyn &dyn) {
+  return __dadd_rn(r.mass0, __dmul_rn(r.dmassdt, dyn.t));
+}
+
+// plane kernels: 128 threads cover 128 consecutive (j, m) elements of a plane
+__device__ __forceinline__ bool plane_coords(const RepDesc &r, int local, int &m, int &j, int &k) {
+  const int chunk = local % r.nchunk;
+  k = local / r.nchunk;
+  const int t = chunk * 128 + (int)threadIdx.x;
+  j = t / r.g.H;
+  m = t - j * r.g.H;
+  return j < r.g.N;
+}
+
+__global__ void __launch_bounds__(128) batch_hb_kernel(const RepDesc *__restrict__ d, const EnsDyn *__restrict__ dyn,
+                                                       const int *__restrict__ rep, const int *__restrict__ first,
+                                                       int phase, int parity, double dt, int ctr_off) {
+  const int r = rep[blockIdx.x];
+  const RepDesc &R = d[r];
+  const EnsDyn y = *dyn;
+  int m, j, k;
+  if (!plane_coords(R, blockIdx.x - first[r], m, j, k)) return;
+  HbArgs a{};
+  a.rdtg = sqrt(2. * dt * R.gamma);
+  a.Lambda2 = 0.5 * (2. * 3. + rep_mass(R, y));
+  a.lam4 = R.lambda / 4.;
+  a.H = R.H;
+  a.sk = sub_key(R.key, y.ctr + (unsigned long long)ctr_off);
+  MonLocal mon;
+  hb_site<false, false>(rep_fields(R, phase, phase), R.g, parity, a, m, j, k, mon);
+}
+
+__global__ void __launch_bounds__(128) batch_charge_kernel(const RepDesc *__restrict__ d,
+                                                           const EnsDyn *__restrict__ dyn, const int *__restrict__ rep,
+                                                           const int *__restrict__ first, int phase, int pass,
+                                                           double dt, int ctr_off_order) {
+  const int r = rep[blockIdx.x];
+  const RepDesc &R = d[r];
+  const EnsDyn y = *dyn;
+  int m, j, k;
+  if (!plane_coords(R, blockIdx.x - first[r], m, j, k)) return;
+  // the replica's pass order (counter mode of ModelGChargeHB::step)
+  const unsigned long long c0 = y.ctr + (unsigned long long)ctr_off_order;
+  const uint64_t w = split_word(sub_key(R.key, c0), 0);
+  const int pi = (int)((w & 0xffffffffull) % 6ull);
+  // lexicographic permutation pi of (0, 1, 2): first element pi / 2, then the
+  // remaining two in order (pi even) or swapped (pi odd)
+  const int p0 = pi / 2;
+  const int lo = (p0 == 0) ? 1 : 0, hi = (p0 == 2) ? 1 : 2;
+  const int ixyz = pass / 2;
+  const int dir = ixyz == 0 ? p0 : (ixyz == 1 ? ((pi & 1) ? hi : lo) : ((pi & 1) ? lo : hi));
+  const int e0 = (int)(w >> 63);
+  const int eoA = (pass & 1) ? (e0 ^ 1) : e0;
+  ChargeArgs a{};
+  a.rms = sqrt(2. * dt * (R.diffusion * R.chi));
+  a.inv2chi = 1.0 / (2. * R.chi);
+  a.sk = sub_key(R.key, c0 + 1 + pass);
+  a.pass = pass;
+  MonLocal mon;
+  charge_link_site<false, false>(rep_fields(R, phase, phase), R.g, dir, eoA, a, m, j, k, mon);
+}
+
+__global__ void __launch_bounds__(128) batch_em_kernel(const RepDesc *__restrict__ d, const EnsDyn *__restrict__ dyn,
+                                                       const int *__restrict__ rep, const int *__restrict__ first,
+                                                       int phase_in, double dt, int ctr_off) {
+  const int r = rep[blockIdx.x];
+  const RepDesc &R = d[r];
+  const EnsDyn y = *dyn;
+  int m, j, k;
+  if (!plane_coords(R, blockIdx.x - first[r], m, j, k)) return;
+  EmArgs a{};
+  a.c6 = 6.0 + rep_mass(R, y);
+  a.dtg = dt * R.gamma;
+  a.sq = sqrt(2.0 * R.gamma * dt);
+  a.lambda = R.lambda;
+  a.H = R.H;
+  a.sk = sub_key(R.key, y.ctr + (unsigned long long)ctr_off);
+  em_pair<false>(rep_fields(R, phase_in, phase_in), rep_fields(R, phase_in ^ 1, phase_in ^ 1), R.g, a, m, j, k);
+}
+
+template <int TX, int TY>
+__global__ void __launch_bounds__(TX *TY, 2) batch_ideal_kernel(const RepDesc *__restrict__ d,
+                                                                const int *__restrict__ rep,
+                                                                const int *__restrict__ first, int pphi, int pq,
+                                                                double dt) {
+  const int r = rep[blockIdx.x];
+  const RepDesc &R = d[r];
+  const int l = blockIdx.x - first[r];
+  const int bx = l % R.igx, by = (l / R.igx) % R.igy, bz = l / (R.igx * R.igy);
+  IdealArgs a;
+  a.dto2chi = (dt / 2.0) / R.chi;
+  a.dt = dt;
+  a.a2 = R.a2;
+  a.H = R.H;
+  ideal_tile<TX, TY>(rep_fields(R, pphi, pq), rep_fields(R, pphi ^ 1, pq ^ 1), R.g, R.izc, a, bx, by, bz);
+}
+
+__global__ void ens_set_kernel(EnsDyn *dyn, unsigned long long ctr, double t) {
+  dyn->ctr = ctr;
+  dyn->t = t;
+}
+__global__ void ens_advance_kernel(EnsDyn *dyn, unsigned long long dctr, double dt) {
+  dyn->ctr += dctr;
+  dyn->t += dt;
+}
+
+// Volume averages of the 11 OAverage observables per replica.
+__global__ void __launch_bounds__(128) batch_oavg_kernel(const RepDesc *__restrict__ d, const int *__restrict__ rep,
+                                                         const int *__restrict__ first, int pphi, int pq,
+                                                         double *partial) {
+  const int r = rep[blockIdx.x];
+  const RepDesc &R = d[r];
+  int m, j, k;
+  double acc[11];
+#pragma unroll
+  for (int o = 0; o < 11; ++o) acc[o] = 0;
+  if (plane_coords(R, blockIdx.x - first[r], m, j, k)) {
+    const long long row = ((long long)k * R.g.N + j) * R.g.H + m;
+#pragma unroll
+    for (int par = 0; par < 2; ++par) {
+      const long long o = par * R.g.V2 + row;
+      double p2 = 0;
+#pragma unroll
+      for (int l = 0; l < 4; ++l) {
+        const double v = R.base[pphi][(long long)l * R.pstride + o];
+        acc[l] += v;
+        p2 += v * v;
+      }
+#pragma unroll
+      for (int l = 4; l < 10; ++l) acc[l] += R.base[pq][(long long)l * R.pstride + o];
+      acc[10] += p2;
+    }
+  }
+  __shared__ double sm[11][4];
+#pragma unroll
+  for (int o = 0; o < 11; ++o) {
+    warp_sum(acc[o]);
+    if ((threadIdx.x & 31) == 0) sm[o][threadIdx.x >> 5] = acc[o];
+  }
+  __syncthreads();
+  if (threadIdx.x < 11) {
+    const int o = threadIdx.x;
+    partial[(long long)blockIdx.x * 11 + o] = ((sm[o][0] + sm[o][1]) + sm[o][2]) + sm[o][3];
+  }
+}
+
+__global__ void batch_oavg_final_kernel(const RepDesc *__restrict__ d, const int *__restrict__ first, int nrep,
+                                        const int *__restrict__ count, const double *partial, double *out) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nrep * 11) return;
+  const int r = t / 11, o = t % 11;
+  double s = 0;
+  for (int b = 0; b < count[r]; ++b) s += partial[(long long)(first[r] + b) * 11 + o];
+  out[t] = s / (2.0 * (double)d[r].g.V2);
+}
+
 inline unsigned nblocks(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
 
 }  // namespace
@@ -1452,6 +1641,76 @@ cudaError_t launch_measure_finish(const double *T, const double *U, int N, doubl
   const int NK = N / 2 + 1;
   meas_dft_kernel<<<nblocks(3LL * kNObs * NK, 128), 128, 0, st>>>(N, mo);
   meas_rotate_kernel<<<nblocks(3LL * NK, 128), 128, 0, st>>>(N, mo);
+  return cudaGetLastError();
+}
+
+
+// ---------------------------------------------------------------------------
+// Batched launchers.
+int ideal_tile_dims(int tile, int *tx, int *ty) {
+  if (tile == LGV_TILE_16x16) {
+    *tx = 16;
+    *ty = 16;
+  } else {
+    *tx = 32;
+    *ty = 8;
+  }
+  return 0;
+}
+
+cudaError_t launch_batch_ideal(const RepDesc *d, const int *rep, const int *first, int nblocks, int tile,
+                               int phase_phi, int phase_q, double dt, cudaStream_t st) {
+  cudaError_t e;
+  if (tile == LGV_TILE_16x16) {
+    using T = IdealTile<16, 16>;
+    if ((e = allow_smem(batch_ideal_kernel<16, 16>, T::SMEM)) != cudaSuccess) return e;
+    batch_ideal_kernel<16, 16><<<nblocks, 256, T::SMEM, st>>>(d, rep, first, phase_phi, phase_q, dt);
+  } else {
+    using T = IdealTile<32, 8>;
+    if ((e = allow_smem(batch_ideal_kernel<32, 8>, T::SMEM)) != cudaSuccess) return e;
+    batch_ideal_kernel<32, 8><<<nblocks, 256, T::SMEM, st>>>(d, rep, first, phase_phi, phase_q, dt);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_hb(const RepDesc *d, const EnsDyn *dyn, const int *rep, const int *first, int nblocks,
+                            int phase, int parity, double dt, int ctr_off, cudaStream_t st) {
+  batch_hb_kernel<<<nblocks, 128, 0, st>>>(d, dyn, rep, first, phase, parity, dt, ctr_off);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_charge(const RepDesc *d, const EnsDyn *dyn, const int *rep, const int *first, int nblocks,
+                                int phase, int pass, double dt, int ctr_off_order, cudaStream_t st) {
+  batch_charge_kernel<<<nblocks, 128, 0, st>>>(d, dyn, rep, first, phase, pass, dt, ctr_off_order);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_em(const RepDesc *d, const EnsDyn *dyn, const int *rep, const int *first, int nblocks,
+                            int phase_in, double dt, int ctr_off, cudaStream_t st) {
+  batch_em_kernel<<<nblocks, 128, 0, st>>>(d, dyn, rep, first, phase_in, dt, ctr_off);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ens_set(EnsDyn *dyn, unsigned long long ctr, double t, cudaStream_t st) {
+  ens_set_kernel<<<1, 1, 0, st>>>(dyn, ctr, t);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ens_advance(EnsDyn *dyn, unsigned long long dctr, double dt, cudaStream_t st) {
+  ens_advance_kernel<<<1, 1, 0, st>>>(dyn, dctr, dt);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_oavg(const RepDesc *d, const int *rep, const int *first, int nblocks, int phase_phi,
+                              int phase_q, double *partial, int nrep, double *out, cudaStream_t st) {
+  // per-replica block counts sit after the partial sums: count[r] = first[r+1] - first[r] in map order
+  batch_oavg_kernel<<<nblocks, 128, 0, st>>>(d, rep, first, phase_phi, phase_q, partial);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_oavg_final(const RepDesc *d, const int *first, const int *count, int nrep,
+                                    const double *partial, double *out, cudaStream_t st) {
+  batch_oavg_final_kernel<<<nblocks((long long)nrep * 11, 128), 128, 0, st>>>(d, first, nrep, count, partial, out);
   return cudaGetLastError();
 }
 
