@@ -59,6 +59,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     return ap.parse_args()
 
 
@@ -246,6 +247,72 @@ def run_ensemble(steps=20, plain_steps=2):
     }
 
 
+ADJ = dict(N=48, steps=2000, avg_begin=1000, ckpt=50, dt=0.02, mass0=-4.813, lam=10.0, H=0.01, gamma=1.0)
+
+
+def run_adjoint(reps=3):
+    """Differentiable Euler-Maruyama Model A at 48^3: 2000 steps, loss averaged
+    over steps 1001..2000, checkpoints every 50 steps.  Times the plain
+    forward (2000 x lgv_step), the differentiable forward (lgv_em_forward:
+    steps + checkpoints + per-step volume averages) and the adjoint
+    (lgv_em_backward: segment recomputation + adjoint kernel) with CUDA events
+    on the handle's stream; best of `reps`."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+    from langevina_b200 import _lib as L
+
+    lib = L.load()
+    c = ADJ
+    N, S = c["N"], c["steps"]
+    p = L.make_params(N, seed=4242, mass0=c["mass0"], lam=c["lam"], H=c["H"], gamma=c["gamma"])
+    h = C.c_void_p()
+    L.check(lib.lgv_create(C.byref(p), C.byref(h)), "lgv_create")
+    stream = torch.cuda.Stream()
+    L.check(lib.lgv_set_stream(h, C.c_void_p(stream.cuda_stream)), "lgv_set_stream")
+    L.check(lib.lgv_initialize(h, L.INIT_PHI_GAUSSIAN, 0.1), "init phi")
+    obs = np.zeros(2)
+    w = np.ones(2)
+    g = np.zeros(4)
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    def plain():
+        L.check(lib.lgv_step(h, L.MODELA_EM, 1, 1, c["dt"], 0.0, S), "em step")
+
+    def fwd():
+        L.check(lib.lgv_em_forward(h, c["dt"], 0.0, S, c["avg_begin"], c["ckpt"], L.ptr(obs)), "em_forward")
+
+    def bwd():
+        L.check(lib.lgv_em_backward(h, L.ptr(w), L.ptr(g)), "em_backward")
+
+    fwd(), bwd(), plain()  # warm-up (allocations, first launches)
+    t_plain, t_fwd, t_bwd = [], [], []
+    for _ in range(reps):
+        t_plain.append(timed(plain))
+        t_fwd.append(timed(fwd))
+        t_bwd.append(timed(bwd))
+    lib.lgv_destroy(h)
+    tp, tf, tb = min(t_plain), min(t_fwd), min(t_bwd)
+    return {
+        "workload": f"Euler-Maruyama Model A {N}^3 FP64, {S} steps, dt={c['dt']}, loss = time average over steps "
+                    f"{c['avg_begin'] + 1}..{S} of sigma + V sum_a pibar_a^2, checkpoints every {c['ckpt']} steps, "
+                    f"m^2={c['mass0']}, lambda={c['lam']}, H={c['H']}, Gamma={c['gamma']}",
+        "plain_forward_ms": tp, "diff_forward_ms": tf, "adjoint_ms": tb,
+        "adjoint_over_forward": tb / tp, "forward_plus_adjoint_over_forward": (tf + tb) / tp,
+        "gradients_per_s": 1e3 / (tf + tb), "grad": g.tolist(), "obs": obs.tolist(),
+        "timing": "CUDA events on the handle's stream, best of %d" % reps,
+    }
+
+
 def run_ours(a):
     import ctypes as C
 
@@ -392,6 +459,9 @@ def run_ours(a):
     ensemble = None
     if world == 1 and not a.no_ensemble:
         ensemble = run_ensemble()
+    adjoint = None
+    if world == 1 and not a.no_adjoint:
+        adjoint = run_adjoint()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -411,6 +481,7 @@ def run_ours(a):
         "cpu_baseline": cpu,
         "e2e": e2e,
         "ensemble": ensemble,
+        "adjoint": adjoint,
         "gpu_launches": launches,
         "clocks": ck,
     }

@@ -219,6 +219,28 @@ int lgv_debug_flags(lgv_handle *h, int enable);
 int lgv_get_flags(lgv_handle *h, uint8_t *host_out);
 
 /* ---------------------------------------------------------------------------
+ * Differentiable Euler-Maruyama Model A.  No counterpart in the reference (it
+ * has no Euler-Maruyama stepper and no gradients); built on the same step as
+ * LGV_MODELA_EM.  lgv_em_forward runs S = nsteps steps of size dt from time t
+ * with the counter noise (the noise is fixed by seed and counter), keeps a
+ * copy of phi every ckpt_every steps and returns two time averages over the
+ * steps n = b+1 .. S (b = avg_begin, M = S - b):
+ *   obs[0] = 1/M sum_n sigma(n)                          sigma = <phi_0>
+ *   obs[1] = 1/M sum_n V sum_{a=1..3} pibar_a(n)^2      pibar_a = <phi_a>
+ * (<.> the volume average, obs[1] the zero-momentum pi equal-time correlator).
+ * The lattice is left at the final state and the counter advanced by S.
+ * lgv_em_backward returns in grad[4] the derivative of w[0]*obs[0] +
+ * w[1]*obs[1] with respect to (mass0, lambda, H, gamma), the noise held
+ * fixed, by the hand-written adjoint of the step; each checkpoint segment is
+ * recomputed with the forward's noise.  Counter noise mode only. */
+int lgv_em_forward(lgv_handle *h, double dt, double t, int nsteps, int avg_begin, int ckpt_every, double *obs);
+int lgv_em_backward(lgv_handle *h, const double *w, double *grad);
+/* The volume averages <phi_a>(n), n = 0..nsteps, a = 0..3, of the last
+ * lgv_em_forward (out holds (nsteps+1)*4 doubles; nsteps must be the
+ * forward's). */
+int lgv_em_averages(lgv_handle *h, double *out, int nsteps);
+
+/* ---------------------------------------------------------------------------
  * Batched ensembles.  Replaces running an ensemble as separate processes or
  * events, one lattice at a time (eventmode loop SuperPions.cxx:228-235, SLURM
  * job arrays grunner.py:153-241): nrep independent replicas, each with its own

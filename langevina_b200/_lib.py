@@ -82,6 +82,9 @@ SIGNATURES = [
     ("lgv_debug_flags", C.c_int, [_H, C.c_int]),
     ("lgv_get_flags", C.c_int, [_H, C.c_void_p]),
     ("lgv_measure_aos_noalloc", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    ("lgv_em_forward", C.c_int, [_H, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, C.c_void_p]),
+    ("lgv_em_backward", C.c_int, [_H, C.c_void_p, C.c_void_p]),
+    ("lgv_em_averages", C.c_int, [_H, C.c_void_p, C.c_int]),
     ("lgv_ensemble_create", C.c_int, [C.c_int, C.c_void_p, C.POINTER(_H)]),
     ("lgv_ensemble_destroy", C.c_int, [_H]),
     ("lgv_ensemble_size", C.c_int, [_H, C.POINTER(C.c_int)]),

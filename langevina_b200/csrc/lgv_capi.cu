@@ -8,6 +8,7 @@
 // or failed kernel surfaces as LGV_ERR_CUDA.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -103,6 +104,19 @@ struct lgv_handle {
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_used;
   double t_ms[LGV_NKCLASS] = {0};
   int64_t t_n[LGV_NKCLASS] = {0};
+  // differentiable Euler-Maruyama run (lgv_em_forward / lgv_em_backward)
+  struct {
+    bool ready = false;
+    lgv_params p{};  // parameters and key of the forward run, used by the backward
+    uint64_t key = 0;
+    double dt = 0;
+    int S = 0, b = 0, K = 1;
+    uint64_t ctr0 = 0;
+    std::vector<double> tn, avg;
+    double *ckpt = nullptr, *seg = nullptr, *lam = nullptr, *avg_dev = nullptr, *partial = nullptr, *g4 = nullptr;
+    unsigned *done = nullptr;  // grid_sum4 counter, zero between launches
+    size_t ckpt_len = 0, seg_len = 0, avg_len = 0, lam_len = 0;
+  } adj;
 };
 
 namespace {
@@ -443,6 +457,9 @@ int lgv_destroy(lgv_handle *h) {
     if (b) cudaFree(b);
   if (h->mon_dev) cudaFree(h->mon_dev);
   if (h->flags_dev) cudaFree(h->flags_dev);
+  for (double *b : {h->adj.ckpt, h->adj.seg, h->adj.lam, h->adj.avg_dev, h->adj.partial, h->adj.g4})
+    if (b) cudaFree(b);
+  if (h->adj.done) cudaFree(h->adj.done);
   for (auto &u : h->ev_used) {
     cudaEventDestroy(u.second.first);
     cudaEventDestroy(u.second.second);
@@ -713,6 +730,177 @@ int lgv_timing_read(lgv_handle *h, int kclass, double *total_ms, int64_t *launch
   h->ev_used.clear();
   *total_ms = h->t_ms[kclass];
   *launches = h->t_n[kclass];
+  return LGV_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Differentiable Euler-Maruyama Model A run.
+namespace {
+
+int adj_realloc(double **p, size_t *len, size_t n) {
+  if (*p && *len >= n) return LGV_OK;
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  *len = 0;
+  LGV_TRY(ensure(p, n));
+  *len = n;
+  return LGV_OK;
+}
+
+Fields phi_slot(double *base, size_t V, size_t slot) {
+  Fields f{};
+  for (int l = 0; l < 4; ++l) f.c[l] = base + (slot * 4 + l) * V;
+  return f;
+}
+
+// the reduction buffers of the differentiable run: CTA partials, the
+// grid_sum4 counter (zeroed once, re-armed by the kernels) and g4
+int adj_counters(lgv_handle *h) {
+  auto &A = h->adj;
+  if (!A.partial) LGV_TRY(ensure(&A.partial, lgv::em_reduce_blocks(h->N) * 4));
+  if (!A.g4) LGV_TRY(ensure(&A.g4, 4));
+  if (!A.done) {
+    LGV_CK(cudaMalloc((void **)&A.done, sizeof(unsigned)));
+    LGV_CK(cudaMemsetAsync(A.done, 0, sizeof(unsigned), h->stream));
+  }
+  return LGV_OK;
+}
+
+// arguments of Euler-Maruyama step number ctr at time t (counter noise), as sub_em builds them
+lgv::EmArgs em_args(const lgv_params &p, uint64_t key, uint64_t ctr, double dt, double t) {
+  lgv::EmArgs e{};
+  e.c6 = 6.0 + (p.mass0 + p.dmassdt * t);
+  e.dtg = dt * p.gamma;
+  e.sq = std::sqrt(2.0 * p.gamma * dt);
+  e.lambda = p.lambda;
+  e.H = p.H;
+  e.sk = lgv::sub_key(key, ctr);
+  return e;
+}
+
+}  // namespace
+
+int lgv_em_forward(lgv_handle *h, double dt, double t, int nsteps, int avg_begin, int ckpt_every, double *obs) {
+  if (!h || !obs) return fail(LGV_ERR_INVALID, "NULL argument");
+  if (nsteps < 1 || avg_begin < 0 || avg_begin >= nsteps || ckpt_every < 1)
+    return fail(LGV_ERR_INVALID, "lgv_em_forward: need nsteps >= 1, 0 <= avg_begin < nsteps, ckpt_every >= 1");
+  if (h->noise_mode != LGV_NOISE_COUNTER) return fail(LGV_ERR_STATE, "lgv_em_forward needs counter noise");
+  DeviceGuard g(h->device);
+  auto &A = h->adj;
+  A.ready = false;
+  const size_t V = h->V;
+  const int S = nsteps, K = ckpt_every;
+  const size_t nck = (size_t)(S - 1) / K + 1;
+  LGV_TRY(adj_realloc(&A.ckpt, &A.ckpt_len, nck * 4 * V));
+  LGV_TRY(adj_realloc(&A.avg_dev, &A.avg_len, (size_t)(S + 1) * 4));
+  LGV_TRY(adj_counters(h));
+  A.dt = dt;
+  A.S = S;
+  A.b = avg_begin;
+  A.K = K;
+  A.ctr0 = h->ctr;
+  A.p = h->p;
+  A.key = h->key;
+  A.tn.assign(S + 1, 0.0);
+  A.tn[0] = t;
+  for (int n = 0; n < S; ++n) A.tn[n + 1] = A.tn[n] + dt;
+  LGV_CK(lgv::launch_phi_avg(h->cur, h->N, A.partial, A.done, A.avg_dev, h->stream));
+  {
+    KTimer tm(h, LGV_KCLASS_EM);
+    for (int n = 0; n < S; ++n) {
+      if (n % K == 0)
+        for (int l = 0; l < 4; ++l)
+          LGV_CK(cudaMemcpyAsync(A.ckpt + ((size_t)(n / K) * 4 + l) * V, h->cur.c[l], V * sizeof(double),
+                                 cudaMemcpyDeviceToDevice, h->stream));
+      const lgv::EmArgs e = em_args(A.p, A.key, A.ctr0 + (uint64_t)n, dt, A.tn[n]);
+      LGV_CK(lgv::launch_em_avg(h->cur, h->alt, h->N, e, A.partial, A.done, A.avg_dev + (size_t)(n + 1) * 4,
+                                h->stream));
+      for (int l = 0; l < 4; ++l) std::swap(h->cur.c[l], h->alt.c[l]);
+    }
+  }
+  h->ctr += (uint64_t)S;
+  A.avg.assign((size_t)(S + 1) * 4, 0.0);
+  LGV_CK(cudaMemcpyAsync(A.avg.data(), A.avg_dev, A.avg.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  LGV_CK(cudaStreamSynchronize(h->stream));
+  // obs[0] = (1/M) sum_{n=b+1}^{S} sigma(n),  obs[1] = (1/M) sum_{n=b+1}^{S} V sum_{a=1..3} pibar_a(n)^2,
+  // M = S - b, sigma and pibar_a the volume averages of phi_0 and phi_a after step n
+  const double Vd = (double)V;
+  double o0 = 0, o1 = 0;
+  for (int n = avg_begin + 1; n <= S; ++n) {
+    const double *a = &A.avg[(size_t)n * 4];
+    o0 += a[0];
+    o1 += Vd * (a[1] * a[1] + a[2] * a[2] + a[3] * a[3]);
+  }
+  obs[0] = o0 / (double)(S - avg_begin);
+  obs[1] = o1 / (double)(S - avg_begin);
+  A.ready = true;
+  return LGV_OK;
+}
+
+int lgv_em_averages(lgv_handle *h, double *out, int nsteps) {
+  if (!h || !out) return fail(LGV_ERR_INVALID, "NULL argument");
+  if (!h->adj.ready) return fail(LGV_ERR_STATE, "lgv_em_averages: no forward run");
+  if (nsteps != h->adj.S) return fail(LGV_ERR_INVALID, "lgv_em_averages: nsteps %d != forward's %d", nsteps, h->adj.S);
+  std::copy(h->adj.avg.begin(), h->adj.avg.end(), out);
+  return LGV_OK;
+}
+
+int lgv_em_backward(lgv_handle *h, const double *w, double *grad) {
+  if (!h || !w || !grad) return fail(LGV_ERR_INVALID, "NULL argument");
+  auto &A = h->adj;
+  if (!A.ready) return fail(LGV_ERR_STATE, "lgv_em_backward: no forward run to differentiate");
+  DeviceGuard g(h->device);
+  const size_t V = h->V;
+  const int S = A.S, K = A.K, M = S - A.b;
+  LGV_TRY(adj_realloc(&A.seg, &A.seg_len, (size_t)K * 4 * V));
+  LGV_TRY(adj_realloc(&A.lam, &A.lam_len, 2 * 4 * V));
+  LGV_TRY(adj_counters(h));
+  LGV_CK(cudaMemsetAsync(A.g4, 0, 4 * sizeof(double), h->stream));
+  const double Vd = (double)V;
+  // dJ/dphi_a(x, n) of J = w0 obs0 + w1 obs1: w0 / (M V) for a = 0, w1 2 pibar_a(n) / M for a >= 1
+  auto gl = [&](int n, double out[4]) {
+    for (int a = 0; a < 4; ++a) out[a] = 0;
+    if (n <= A.b) return;
+    const double *av = &A.avg[(size_t)n * 4];
+    out[0] = w[0] / (Vd * M);
+    for (int a = 1; a < 4; ++a) out[a] = w[1] * 2.0 * av[a] / M;
+  };
+  int cur = 0;
+  {
+    double v[4];
+    gl(S, v);
+    LGV_CK(lgv::launch_fill_phi(phi_slot(A.lam, V, 0), h->N, v, h->stream));
+  }
+  int loaded = -1;
+  for (int n = S - 1; n >= 0; --n) {
+    const int s = n / K;
+    if (s != loaded) {
+      // phi_{sK} .. phi_{min(sK+K, S)-1} again from the checkpoint, with the forward's noise
+      for (int l = 0; l < 4; ++l)
+        LGV_CK(cudaMemcpyAsync(A.seg + (size_t)l * V, A.ckpt + ((size_t)s * 4 + l) * V, V * sizeof(double),
+                               cudaMemcpyDeviceToDevice, h->stream));
+      const int last = std::min(s * K + K - 1, S - 1);
+      for (int m = s * K; m < last; ++m) {
+        const lgv::EmArgs e = em_args(A.p, A.key, A.ctr0 + (uint64_t)m, A.dt, A.tn[m]);
+        LGV_CK(lgv::launch_em(phi_slot(A.seg, V, m - s * K), phi_slot(A.seg, V, m - s * K + 1), h->N, e, h->stream));
+      }
+      loaded = s;
+    }
+    lgv::EmAdjArgs a{};
+    a.c6 = 6.0 + (A.p.mass0 + A.p.dmassdt * A.tn[n]);
+    a.dtg = A.dt * A.p.gamma;
+    a.dt = A.dt;
+    a.lambda = A.p.lambda;
+    a.H = A.p.H;
+    a.cxi = std::sqrt(2.0 * A.dt) / (2.0 * std::sqrt(A.p.gamma));
+    gl(n, a.gl);
+    a.sk = lgv::sub_key(A.key, A.ctr0 + (uint64_t)n);
+    LGV_CK(lgv::launch_em_adjoint(phi_slot(A.seg, V, n - s * K), phi_slot(A.lam, V, cur), phi_slot(A.lam, V, cur ^ 1),
+                                  h->N, a, A.partial, A.done, A.g4, h->stream));
+    cur ^= 1;
+  }
+  LGV_CK(cudaMemcpyAsync(grad, A.g4, 4 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  LGV_CK(cudaStreamSynchronize(h->stream));
   return LGV_OK;
 }
 

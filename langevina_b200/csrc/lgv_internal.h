@@ -106,6 +106,34 @@ cudaError_t launch_batch_oavg_final(const RepDesc *d, const int *first, const in
                                     const double *partial, double *out, cudaStream_t st);
 int ideal_tile_dims(int tile, int *tx, int *ty);
 
+// ---------------------------------------------------------------------------
+// Adjoint of the Euler-Maruyama Model A step (noise held fixed).
+struct EmAdjArgs {
+  double c6;      // 6 + m^2
+  double dtg;     // dt * gamma
+  double dt;
+  double lambda;
+  double H;
+  double cxi;     // d sqrt(2 gamma dt) / d gamma = sqrt(2 dt) / (2 sqrt(gamma))
+  double gl[4];   // uniform loss gradient dL/dphi_a added to the adjoint of this state
+  uint64_t sk;    // the step's noise key (regenerates xi)
+};
+// lam_out = J^T lam_in + gl at state phi; per-block parameter-gradient partial
+// sums (dm2, dlambda, dH, dgamma) into partial[nblocks][4]
+// Euler-Maruyama step that also writes the volume averages of the new phi
+// to avg_out[0..3]; partial holds em_reduce_blocks(N) * 4 doubles and *done
+// is a zeroed counter (left zeroed).
+cudaError_t launch_em_avg(Fields in, Fields out, int N, const EmArgs &a, double *partial, unsigned *done,
+                          double *avg_out, cudaStream_t st);
+size_t em_reduce_blocks(int N);
+// adjoint of one Euler-Maruyama step; adds dL/d(m^2, lambda, H, Gamma) of the step into g4[0..3]
+cudaError_t launch_em_adjoint(Fields phi, Fields lam_in, Fields lam_out, int N, const EmAdjArgs &a, double *partial,
+                              unsigned *done, double *g4, cudaStream_t st);
+// volume averages of phi_0..3 -> out[4]
+cudaError_t launch_phi_avg(Fields f, int N, double *partial, unsigned *done, double *out, cudaStream_t st);
+// phi planes of f set to the constants v[4]
+cudaError_t launch_fill_phi(Fields f, int N, const double v[4], cudaStream_t st);
+
 // Launchers (lgv_kernels.cu).  All asynchronous on `st`; return cudaError_t.
 cudaError_t launch_aos_to_rb(const double *aos, Fields f, int N, cudaStream_t st);
 cudaError_t launch_rb_to_aos(Fields f, double *aos, int N, cudaStream_t st);

@@ -16,6 +16,7 @@
 //                       computeDerivedObs (measurer.cxx:10-317)
 #include "lgv_internal.h"
 
+#include <algorithm>
 #include <cstdio>
 
 namespace lgv {
@@ -31,6 +32,55 @@ __device__ __forceinline__ void warp_sum(double &v) {
 __device__ __forceinline__ void warp_sum(unsigned long long &v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+}
+
+// Sums v[0..3] over the CTA into partial[blockIdx.x][0..3]; the last CTA of
+// the grid to finish then adds the CTA partials in block order (fixed, so the
+// result does not depend on which CTA ends last), scaled, into out[0..3]
+// (accumulating when add) and re-arms the counter.  `done` is zero on entry.
+template <int NT>
+__device__ __forceinline__ void grid_sum4(double (&v)[4], double *partial, unsigned *done, double *out, double scale,
+                                          bool add) {
+  static_assert(NT % 32 == 0 && NT >= 128, "grid_sum4: NT");
+  constexpr int NW = NT / 32;
+  __shared__ double sm[4][NW];
+  __shared__ bool last;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    warp_sum(v[q]);
+    if (lane == 0) sm[q][warp] = v[q];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      double t = 0;
+#pragma unroll
+      for (int w = 0; w < NW; ++w) t += sm[q][w];
+      partial[(size_t)blockIdx.x * 4 + q] = t;
+    }
+    __threadfence();
+    last = atomicAdd(done, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  if (warp < 4) {
+    double t = 0;
+    for (unsigned b = lane; b < gridDim.x; b += 32) t += __ldcg(partial + (size_t)b * 4 + warp);
+    warp_sum(t);
+    if (lane == 0) out[warp] = add ? out[warp] + t * scale : t * scale;
+  }
+  if (threadIdx.x == 0) *done = 0u;
+}
+
+// Flat site-pair index -> (m, j, k) of the red-black half rows: idx = (k N + j) H + m.
+__device__ __forceinline__ void pair_coords(long long idx, const Geo &g, int &m, int &j, int &k) {
+  const long long row = idx / g.H;
+  m = (int)(idx - row * g.H);
+  k = (int)(row / g.N);
+  j = (int)(row - (long long)k * g.N);
 }
 
 // Per-thread monitor tally, reduced per block and added once per block.
@@ -714,7 +764,7 @@ __global__ void __launch_bounds__(128) charge_line_kernel(Fields in, Fields out,
 // One thread per element m of both parity half-rows of row (j, k).
 template <bool INJECTED>
 __device__ __forceinline__ void em_pair(const Fields &in, const Fields &out, const Geo &g, const EmArgs &a, int m,
-                                        int j, int k) {
+                                        int j, int k, double (&acc)[4]) {
   const int H = g.H, N = g.N;
   const long long row = ((long long)k * N + j) * H;
   const long long rjp = ((long long)k * N + wrap_inc(j, N)) * H;
@@ -752,15 +802,27 @@ __device__ __forceinline__ void em_pair(const Fields &in, const Fields &out, con
                           (P[ob + rkp + m] + P[ob + rkm + m]);
       double fo = -heff + a.c6 * c[l] + a.lambda * p2 * c[l];
       if (l == 0) fo -= a.H;
-      out.c[l][own] = c[l] - a.dtg * fo + a.sq * xi[l];
+      const double v = c[l] - a.dtg * fo + a.sq * xi[l];
+      out.c[l][own] = v;
+      acc[l] += v;
     }
   }
 }
 
-template <bool INJECTED>
-__global__ void __launch_bounds__(128) em_kernel(Fields in, Fields out, Geo g, EmArgs a) {
-  const int m = blockIdx.x * blockDim.x + threadIdx.x;
-  if (m < g.H) em_pair<INJECTED>(in, out, g, a, m, blockIdx.y, blockIdx.z);
+// One thread per site pair (element m of both parity half rows of row (j, k)),
+// flat over the V/2 pairs.  AVG: also the volume averages of the new phi into
+// avg_out[0..3] (grid_sum4).
+template <bool INJECTED, bool AVG>
+__global__ void __launch_bounds__(kThreads) em_kernel(Fields in, Fields out, Geo g, EmArgs a, double *partial,
+                                                      unsigned *done, double *avg_out) {
+  const long long idx = (long long)blockIdx.x * kThreads + threadIdx.x;
+  double acc[4] = {0, 0, 0, 0};
+  if (idx < g.V2) {
+    int m, j, k;
+    pair_coords(idx, g, m, j, k);
+    em_pair<INJECTED>(in, out, g, a, m, j, k, acc);
+  }
+  if (AVG) grid_sum4<kThreads>(acc, partial, done, avg_out, 1.0 / (2.0 * (double)g.V2), false);
 }
 
 // ----------------------------------------------------------------------------
@@ -1314,7 +1376,8 @@ __global__ void __launch_bounds__(128) batch_em_kernel(const RepDesc *__restrict
   a.lambda = R.lambda;
   a.H = R.H;
   a.sk = sub_key(R.key, y.ctr + (unsigned long long)ctr_off);
-  em_pair<false>(rep_fields(R, phase_in, phase_in), rep_fields(R, phase_in ^ 1, phase_in ^ 1), R.g, a, m, j, k);
+  double acc[4] = {0, 0, 0, 0};
+  em_pair<false>(rep_fields(R, phase_in, phase_in), rep_fields(R, phase_in ^ 1, phase_in ^ 1), R.g, a, m, j, k, acc);
 }
 
 template <int TX, int TY>
@@ -1391,6 +1454,98 @@ __global__ void batch_oavg_final_kernel(const RepDesc *__restrict__ d, const int
   double s = 0;
   for (int b = 0; b < count[r]; ++b) s += partial[(long long)(first[r] + b) * 11 + o];
   out[t] = s / (2.0 * (double)d[r].g.V2);
+}
+
+// ----------------------------------------------------------------------------
+// Adjoint of the Euler-Maruyama step (noise fixed).  The step is
+//   phi'_a = phi_a - dt G F_a(phi) + sqrt(2 G dt) xi_a,
+//   F_a = -sum_nbr phi_a + (6 + m^2) phi_a + lambda phi^2 phi_a - H delta_a0,
+// so with lam = dL/dphi' (lam_in) the adjoint of the state is
+//   lam_b - dt G [(6 + m^2) lam_b + lambda (phi^2 lam_b + 2 phi_b (phi . lam))
+//                 - sum_nbr lam_b] + gl_b
+// (the lattice Laplacian is symmetric), and the parameter sensitivities are
+//   dL/dm^2 += -dtG (phi . lam),  dL/dlambda += -dtG phi^2 (phi . lam),
+//   dL/dH += dtG lam_0,  dL/dG += lam . (-dt F + sqrt(2dt)/(2 sqrt G) xi).
+// One thread per site pair, flat over the V/2 pairs; the parameter sums are
+// accumulated into g4[0..3] (grid_sum4).
+constexpr int kAdjThreads = 128;
+__global__ void __launch_bounds__(kAdjThreads, 4) em_adjoint_kernel(Fields phi, Fields lin, Fields lout, Geo g,
+                                                                 EmAdjArgs a, double *partial, unsigned *done,
+                                                                 double *g4) {
+  const long long idx = (long long)blockIdx.x * kAdjThreads + threadIdx.x;
+  const int H = g.H, N = g.N;
+  double gm = 0, gla = 0, gh = 0, gg = 0;
+  if (idx < g.V2) {
+    int m, j, k;
+    pair_coords(idx, g, m, j, k);
+    const long long row = ((long long)k * N + j) * H;
+    const long long rjp = ((long long)k * N + wrap_inc(j, N)) * H;
+    const long long rjm = ((long long)k * N + wrap_dec(j, N)) * H;
+    const long long rkp = ((long long)wrap_inc(k, N) * N + j) * H;
+    const long long rkm = ((long long)wrap_dec(k, N) * N + j) * H;
+#pragma unroll
+    for (int parity = 0; parity < 2; ++parity) {
+      const int s = (parity + j + k) & 1;
+      int xm = m - 1 + s, xp = m + s;
+      if (xm < 0) xm += H;
+      if (xp == H) xp = 0;
+      const long long own = (long long)parity * g.V2 + row + m;
+      const long long ob = (long long)(parity ^ 1) * g.V2;
+      const long long nat = ((long long)k * N + j) * N + 2 * m + s;
+      double c[4], l[4];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        c[b] = phi.c[b][own];
+        l[b] = lin.c[b][own];
+      }
+      Xoro rng = stream_at(a.sk, (uint64_t)nat);
+      double xi[4];
+      const uint64_t r1 = rng.next(), r2 = rng.next(), r3 = rng.next(), r4 = rng.next();
+      box_muller(r1, r2, xi[0], xi[1]);
+      box_muller(r3, r4, xi[2], xi[3]);
+      const double p2 = c[0] * c[0] + c[1] * c[1] + c[2] * c[2] + c[3] * c[3];
+      const double dot = c[0] * l[0] + c[1] * l[1] + c[2] * l[2] + c[3] * l[3];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        const double *P = phi.c[b], *Lm = lin.c[b];
+        const double hf = (P[ob + row + xp] + P[ob + row + xm]) + (P[ob + rjp + m] + P[ob + rjm + m]) +
+                          (P[ob + rkp + m] + P[ob + rkm + m]);
+        const double nl = (Lm[ob + row + xp] + Lm[ob + row + xm]) + (Lm[ob + rjp + m] + Lm[ob + rjm + m]) +
+                          (Lm[ob + rkp + m] + Lm[ob + rkm + m]);
+        const double jl = a.c6 * l[b] + a.lambda * (p2 * l[b] + 2.0 * c[b] * dot) - nl;
+        lout.c[b][own] = l[b] - a.dtg * jl + a.gl[b];
+        double F = -hf + a.c6 * c[b] + a.lambda * p2 * c[b];
+        if (b == 0) F -= a.H;
+        gg += l[b] * (-a.dt * F + a.cxi * xi[b]);
+      }
+      gm += -a.dtg * dot;
+      gla += -a.dtg * p2 * dot;
+      gh += a.dtg * l[0];
+    }
+  }
+  double v[4] = {gm, gla, gh, gg};
+  grid_sum4<kAdjThreads>(v, partial, done, g4, 1.0, true);
+}
+
+// volume averages of phi_0..3 into out[0..3]
+__global__ void __launch_bounds__(kThreads) phi_avg_kernel(Fields f, Geo g, double *partial, unsigned *done,
+                                                           double *out) {
+  const long long idx = (long long)blockIdx.x * kThreads + threadIdx.x;
+  double v[4] = {0, 0, 0, 0};
+  if (idx < g.V2) {
+#pragma unroll
+    for (int b = 0; b < 4; ++b) v[b] = f.c[b][idx] + f.c[b][g.V2 + idx];
+  }
+  grid_sum4<kThreads>(v, partial, done, out, 1.0 / (2.0 * (double)g.V2), false);
+}
+
+__global__ void fill_phi_kernel(Fields f, long long V, double v0, double v1, double v2, double v3) {
+  const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= V) return;
+  f.c[0][n] = v0;
+  f.c[1][n] = v1;
+  f.c[2][n] = v2;
+  f.c[3][n] = v3;
 }
 
 inline unsigned nblocks(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
@@ -1570,9 +1725,18 @@ cudaError_t launch_charge_dir(Fields in, Fields out, int N, int dir, const Charg
 
 cudaError_t launch_em(Fields in, Fields out, int N, const EmArgs &a, cudaStream_t st) {
   const Geo g = make_geo(N);
-  dim3 grid((g.H + 127) / 128, N, N);
-  if (a.xi) em_kernel<true><<<grid, 128, 0, st>>>(in, out, g, a);
-  else em_kernel<false><<<grid, 128, 0, st>>>(in, out, g, a);
+  const unsigned nb = nblocks(g.V2, kThreads);
+  if (a.xi) em_kernel<true, false><<<nb, kThreads, 0, st>>>(in, out, g, a, nullptr, nullptr, nullptr);
+  else em_kernel<false, false><<<nb, kThreads, 0, st>>>(in, out, g, a, nullptr, nullptr, nullptr);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_em_avg(Fields in, Fields out, int N, const EmArgs &a, double *partial, unsigned *done,
+                          double *avg_out, cudaStream_t st) {
+  const Geo g = make_geo(N);
+  const unsigned nb = nblocks(g.V2, kThreads);
+  if (a.xi) em_kernel<true, true><<<nb, kThreads, 0, st>>>(in, out, g, a, partial, done, avg_out);
+  else em_kernel<false, true><<<nb, kThreads, 0, st>>>(in, out, g, a, partial, done, avg_out);
   return cudaGetLastError();
 }
 
@@ -1711,6 +1875,35 @@ cudaError_t launch_batch_oavg(const RepDesc *d, const int *rep, const int *first
 cudaError_t launch_batch_oavg_final(const RepDesc *d, const int *first, const int *count, int nrep,
                                     const double *partial, double *out, cudaStream_t st) {
   batch_oavg_final_kernel<<<nblocks((long long)nrep * 11, 128), 128, 0, st>>>(d, first, nrep, count, partial, out);
+  return cudaGetLastError();
+}
+
+
+// ---------------------------------------------------------------------------
+// Euler-Maruyama adjoint launchers.
+size_t em_reduce_blocks(int N) {
+  const Geo g = make_geo(N);
+  return std::max<size_t>(nblocks(g.V2, kThreads), nblocks(g.V2, kAdjThreads));
+}
+
+cudaError_t launch_em_adjoint(Fields phi, Fields lam_in, Fields lam_out, int N, const EmAdjArgs &a, double *partial,
+                              unsigned *done, double *g4, cudaStream_t st) {
+  const Geo g = make_geo(N);
+  em_adjoint_kernel<<<nblocks(g.V2, kAdjThreads), kAdjThreads, 0, st>>>(phi, lam_in, lam_out, g, a, partial, done,
+                                                                         g4);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_phi_avg(Fields f, int N, double *partial, unsigned *done, double *out, cudaStream_t st) {
+  const Geo g = make_geo(N);
+  phi_avg_kernel<<<nblocks(g.V2, kThreads), kThreads, 0, st>>>(f, g, partial, done, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fill_phi(Fields f, int N, const double v[4], cudaStream_t st) {
+  const Geo g = make_geo(N);
+  const long long V = 2 * g.V2;
+  fill_phi_kernel<<<nblocks(V, 256), 256, 0, st>>>(f, V, v[0], v[1], v[2], v[3]);
   return cudaGetLastError();
 }
 

@@ -975,6 +975,18 @@ void orc_ctr_draws(uint64_t seed, uint64_t ctr, uint64_t n, int ndraw, uint64_t 
   orc::CtrStream cs(orc::subkey(orc::make_key(seed), ctr), n);
   for (int i = 0; i < ndraw; ++i) out[i] = cs.next();
 }
+// Counter-mode Euler-Maruyama normals of step counter ctr: xi[l * N^3 + n] for
+// natural site n = (k N + j) N + i, the draws em_step takes in counter mode.
+void orc_em_noise(uint64_t seed, uint64_t ctr, int N, double *xi) {
+  const uint64_t sk = orc::subkey(orc::make_key(seed), ctr);
+  const size_t V = (size_t)N * N * N;
+  for (size_t n = 0; n < V; ++n) {
+    orc::CtrStream cs(sk, n);
+    const uint64_t r1 = cs.next(), r2 = cs.next(), r3 = cs.next(), r4 = cs.next();
+    orc::box_muller(r1, r2, xi[n], xi[V + n]);
+    orc::box_muller(r3, r4, xi[2 * V + n], xi[3 * V + n]);
+  }
+}
 // Charge pass order of a counter-mode charge step at counter ctr.
 void orc_ctr_order(uint64_t seed, uint64_t ctr, int32_t *order5) {
   const uint64_t w = orc::word(orc::subkey(orc::make_key(seed), ctr), 0);

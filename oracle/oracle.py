@@ -67,6 +67,7 @@ def load():
         "orc_seed_seq": (None, [C.c_int, C.c_int, C.c_void_p]),
         "orc_ctr_draws": (None, [C.c_uint64, C.c_uint64, C.c_uint64, C.c_int, C.c_void_p]),
         "orc_ctr_order": (None, [C.c_uint64, C.c_uint64, C.c_void_p]),
+        "orc_em_noise": (None, [C.c_uint64, C.c_uint64, C.c_int, C.c_void_p]),
         "orc_charge_pair_chain": (None, [C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int,
                                          C.c_void_p, C.c_void_p]),
         "orc_last_error": (C.c_char_p, []),
@@ -218,6 +219,14 @@ def ctr_order(seed, ctr):
     lib = load()
     out = np.zeros(5, dtype=np.int32)
     lib.orc_ctr_order(int(seed), int(ctr), _ptr(out))
+    return out
+
+
+def em_noise(seed, ctr, N):
+    """Counter-mode Euler-Maruyama normals of step counter ctr, shape (4, N, N, N) = [l, k, j, i]."""
+    lib = load()
+    out = np.zeros((4, N, N, N))
+    lib.orc_em_noise(int(seed), int(ctr), int(N), _ptr(out))
     return out
 
 

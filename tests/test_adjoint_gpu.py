@@ -1,0 +1,239 @@
+"""GPU checks of the differentiable Euler-Maruyama Model A path
+(lgv_em_forward / lgv_em_backward and the torch.autograd.Function over them).
+
+- the time averages and the adjoint gradient against the numpy restatement of
+  the run and its adjoint (oracle/em_adjoint.py), on the same counter noise;
+- the gradient with respect to (m^2, lambda, H, Gamma) against central finite
+  differences, h = 1e-5, with common random numbers (same state, same seed and
+  counter), within 1e-6 relative: on small lattices and on the 48^3, 2000-step
+  run with checkpoints every 50 steps;
+- at equilibrium, d<sigma>/dH against the fluctuation-dissipation
+  susceptibility V (<sigma^2> - <sigma>^2) of the same trajectories.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from lgvtest import GpuLattice, rand_state
+
+pytestmark = pytest.mark.gpu
+
+SEED = 977
+CFG4 = dict(mass0=-4.813, lam=10.0, H=0.01, gamma=1.0)  # (m^2, lambda, H, Gamma) of the 48^3 run
+
+
+def theta_of(c):
+    return np.array([c["mass0"], c["lam"], c["H"], c["gamma"]])
+
+
+def kw_of(theta):
+    return dict(mass0=float(theta[0]), lam=float(theta[1]), H=float(theta[2]), gamma=float(theta[3]))
+
+
+class EmLattice(GpuLattice):
+    def forward(self, dt, S, b, K, t=0.0):
+        obs = np.zeros(2)
+        self.L.check(self.lib.lgv_em_forward(self.h, float(dt), float(t), int(S), int(b), int(K), self.L.ptr(obs)),
+                     "em_forward")
+        return obs
+
+    def backward(self, w=(1.0, 1.0)):
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        g = np.zeros(4)
+        self.L.check(self.lib.lgv_em_backward(self.h, self.L.ptr(w), self.L.ptr(g)), "em_backward")
+        return g
+
+    def averages(self, S):
+        out = np.zeros((S + 1, 4))
+        self.L.check(self.lib.lgv_em_averages(self.h, self.L.ptr(out), int(S)), "em_averages")
+        return out
+
+    def set_theta(self, theta, **extra):
+        self.p = self.L.make_params(self.N, seed=SEED, **kw_of(theta), **extra)
+        self.L.check(self.lib.lgv_set_params(self.h, C.byref(self.p)), "set_params")
+
+
+def central_fd(lat, u, ctr, theta, run, w=(1.0, 1.0), h=1e-5, **extra):
+    fd = np.zeros(4)
+    for i in range(4):
+        vals = []
+        for sgn in (1.0, -1.0):
+            th = np.array(theta, dtype=np.float64)
+            th[i] += sgn * h
+            lat.set_theta(th, **extra)
+            lat.set_state(u)
+            lat.counter(ctr)
+            vals.append(np.dot(w, lat.forward(*run)))
+        fd[i] = (vals[0] - vals[1]) / (2 * h)
+    lat.set_theta(theta, **extra)
+    return fd
+
+
+def assert_grad_close(g, ref, rtol, what):
+    scale = np.max(np.abs(ref))
+    err = np.abs(g - ref) / np.maximum(np.abs(ref), 1e-3 * scale)
+    assert np.all(err <= rtol), f"{what}: relative errors {err} > {rtol:.0e} (grad {g}, reference {ref})"
+    return err
+
+
+@pytest.mark.parametrize("N,S,b,K", [(8, 40, 15, 7), (6, 25, 0, 25), (10, 33, 32, 4)])
+def test_adjoint_matches_numpy_restatement(lgv, oracle_mod, N, S, b, K):
+    import em_adjoint as ema
+
+    theta = theta_of(CFG4)
+    lat = EmLattice(lgv, N, seed=SEED, dmassdt=-0.3, **kw_of(theta))
+    u = rand_state(N, 3 + N)
+    lat.set_state(u)
+    lat.counter(5)
+    dt, t0 = 0.02, 0.5
+    obs = lat.forward(dt, S, b, K, t=t0)
+    assert lat.counter() == 5 + S
+    phis = ema.em_run(u[..., :4], theta, dt, S, SEED, 5, t0=t0, dmassdt=-0.3)
+    np.testing.assert_allclose(lat.get_state()[..., :4], phis[-1], rtol=1e-12, atol=1e-12)
+    np.testing.assert_array_equal(lat.get_state()[..., 4:], u[..., 4:])
+    np.testing.assert_allclose(obs, ema.observables(phis, b), rtol=1e-12, atol=1e-14)
+    avg = lat.averages(S)
+    np.testing.assert_allclose(avg, np.array([p.mean(axis=(0, 1, 2)) for p in phis]), rtol=1e-12, atol=1e-14)
+    for w in [(1.0, 1.0), (0.5, -2.0), (0.0, 1.0)]:
+        g = lat.backward(w)
+        ref = ema.em_gradient(phis, theta, dt, b, SEED, 5, w=w, t0=t0, dmassdt=-0.3)
+        assert_grad_close(g, ref, 1e-10, f"adjoint vs numpy restatement N={N} w={w}")
+
+
+@pytest.mark.parametrize("N,S,b,K", [(16, 400, 200, 50), (12, 300, 100, 64)])
+def test_adjoint_matches_central_fd_small(lgv, N, S, b, K):
+    theta = theta_of(CFG4)
+    lat = EmLattice(lgv, N, seed=SEED, **kw_of(theta))
+    u = rand_state(N, 21, charges=False)
+    run = (0.02, S, b, K)
+    lat.set_state(u)
+    lat.counter(0)
+    lat.forward(*run)
+    g = lat.backward((1.0, 1.0))
+    fd = central_fd(lat, u, 0, theta, run)
+    assert_grad_close(g, fd, 1e-6, f"adjoint vs central FD N={N}")
+
+
+def test_adjoint_matches_central_fd_48cubed_2000_steps(lgv):
+    """The 48^3 Euler-Maruyama run: 2000 steps, dt = 0.02, loss averaged over
+    steps 1001..2000, checkpoints every 50 steps."""
+    N = 48
+    theta = theta_of(CFG4)
+    lat = EmLattice(lgv, N, seed=SEED, **kw_of(theta))
+    u = rand_state(N, 48, phi_scale=0.1, charges=False)
+    run = (0.02, 2000, 1000, 50)
+    lat.set_state(u)
+    lat.counter(0)
+    lat.forward(*run)
+    g = lat.backward((1.0, 1.0))
+    fd = central_fd(lat, u, 0, theta, run)
+    assert_grad_close(g, fd, 1e-6, "adjoint vs central FD at 48^3")
+
+
+def test_backward_is_repeatable_and_leaves_state(lgv):
+    N = 8
+    lat = EmLattice(lgv, N, seed=SEED, **CFG4)
+    lat.set_state(rand_state(N, 2))
+    lat.forward(0.02, 60, 20, 16)
+    after = lat.get_state()
+    c = lat.counter()
+    g1 = lat.backward((1.0, 1.0))
+    g2 = lat.backward((1.0, 1.0))
+    assert np.array_equal(g1, g2)
+    assert np.array_equal(lat.get_state(), after)
+    assert lat.counter() == c
+    # the gradient is linear in the weights
+    np.testing.assert_allclose(lat.backward((2.0, 0.0)) + lat.backward((0.0, 3.0)),
+                               2 * lat.backward((1.0, 0.0)) + 3 * lat.backward((0.0, 1.0)), rtol=1e-13, atol=1e-15)
+
+
+def test_adjoint_errors(lgv):
+    N = 4
+    lat = EmLattice(lgv, N, seed=SEED, **CFG4)
+    w, g = np.ones(2), np.zeros(4)
+    assert lat.lib.lgv_em_backward(lat.h, lat.L.ptr(w), lat.L.ptr(g)) != 0  # no forward yet
+    obs = np.zeros(2)
+    assert lat.lib.lgv_em_forward(lat.h, 0.02, 0.0, 10, 10, 5, lat.L.ptr(obs)) != 0  # avg_begin == nsteps
+    assert lat.lib.lgv_em_forward(lat.h, 0.02, 0.0, 10, 0, 0, lat.L.ptr(obs)) != 0  # ckpt_every 0
+    lat.mode(1)
+    assert lat.lib.lgv_em_forward(lat.h, 0.02, 0.0, 10, 0, 5, lat.L.ptr(obs)) != 0  # injected noise
+
+
+def _model(lgv, N, theta, seed=SEED):
+    data = lgv.ModelAData(dict(NX=N, mass0=theta[0], **{"lambda": theta[1]}, H=theta[2], gamma=theta[3],
+                               seed=seed, deltat=0.02, finaltime=1.0))
+    return lgv.ModelA(data)
+
+
+def test_autograd_function_gradcheck(lgv):
+    import torch
+
+    from langevina_b200.adjoint import em_observables
+
+    N = 8
+    model = _model(lgv, N, theta_of(CFG4))
+    u = rand_state(N, 9)
+    model.set_state(u)
+
+    def f(theta):
+        model.set_state(u)
+        model.set_counter(4)
+        return em_observables(model, theta, 0.02, 50, 20, ckpt_every=16)
+
+    theta = torch.tensor(theta_of(CFG4), dtype=torch.float64, requires_grad=True)
+    assert torch.autograd.gradcheck(f, (theta,), eps=1e-5, atol=1e-9, rtol=1e-6)
+
+    obs = f(theta)
+    (obs[0] + obs[1]).backward()
+    lat_g = model.em_backward((1.0, 1.0))
+    assert np.array_equal(theta.grad.numpy(), lat_g)
+
+
+def test_autograd_backward_after_another_forward(lgv):
+    import torch
+
+    from langevina_b200.adjoint import em_observables
+
+    N = 8
+    model = _model(lgv, N, theta_of(CFG4))
+    u = rand_state(N, 10)
+    model.set_state(u)
+    model.set_counter(0)
+    th1 = torch.tensor(theta_of(CFG4), dtype=torch.float64, requires_grad=True)
+    o1 = em_observables(model, th1, 0.02, 40, 10, ckpt_every=8)
+    expect = model.em_backward((1.0, 1.0))
+    th2 = torch.tensor(theta_of(CFG4) * 1.01, dtype=torch.float64, requires_grad=True)
+    o2 = em_observables(model, th2, 0.02, 30, 5, ckpt_every=8)
+    state2, ctr2 = model.get_state(), model.get_counter()
+    o1.sum().backward()
+    assert np.array_equal(th1.grad.numpy(), expect)
+    assert np.array_equal(model.get_state(), state2) and model.get_counter() == ctr2
+    o2.sum().backward()
+    assert th2.grad is not None and np.all(np.isfinite(th2.grad.numpy()))
+
+
+def test_fluctuation_dissipation_susceptibility(lgv):
+    """At equilibrium d<sigma>/dH = V (<sigma^2> - <sigma>^2) (the stationary
+    weight is exp(-S) with S linear in -H sum phi_0).  Symmetric phase,
+    m^2 = 1, lambda = 1, H = 0.2, dt = 0.005; 8 seeds of 60000 steps on 8^3,
+    the first 10000 dropped.  The Euler-Maruyama chain's own stationary
+    variance is larger by about dt m_eff^2 / 2 (< 1%); the check allows that
+    plus 4 standard errors over the seeds."""
+    N, S, b, K, dt = 8, 60000, 10000, 500, 0.005
+    theta = np.array([1.0, 1.0, 0.2, 1.0])
+    V = N ** 3
+    adj, fdt = [], []
+    for s in range(8):
+        lat = EmLattice(lgv, N, seed=1000 + s, **kw_of(theta))
+        lat.set_state(np.zeros((N, N, N, 10)))
+        lat.counter(0)
+        lat.forward(dt, S, b, K)
+        adj.append(lat.backward((1.0, 0.0))[2])
+        sig = lat.averages(S)[b + 1:, 0]
+        fdt.append(V * sig.var())
+        lat.close()
+    adj, fdt = np.array(adj), np.array(fdt)
+    ma, mf = adj.mean(), fdt.mean()
+    se = np.sqrt(adj.var(ddof=1) / len(adj) + fdt.var(ddof=1) / len(fdt))
+    assert abs(ma - mf) <= 4 * se + 0.01 * mf, f"d<sigma>/dH {ma:.4f} vs V var(sigma) {mf:.4f} (se {se:.4f})"
