@@ -253,9 +253,9 @@ ADJ = dict(N=48, steps=2000, avg_begin=1000, ckpt=50, dt=0.02, mass0=-4.813, lam
 def run_adjoint(reps=3):
     """Differentiable Euler-Maruyama Model A at 48^3: 2000 steps, loss averaged
     over steps 1001..2000, checkpoints every 50 steps.  Times the plain
-    forward (2000 x lgv_step), the differentiable forward (lgv_em_forward:
+    forward (2000 x lgv_step), the differentiable forward (lgv_diff_forward:
     steps + checkpoints + per-step volume averages) and the adjoint
-    (lgv_em_backward: segment recomputation + adjoint kernel) with CUDA events
+    (lgv_diff_backward: segment recomputation + adjoint kernel) with CUDA events
     on the handle's stream; best of `reps`."""
     import ctypes as C
 
@@ -289,10 +289,11 @@ def run_adjoint(reps=3):
         L.check(lib.lgv_step(h, L.MODELA_EM, 1, 1, c["dt"], 0.0, S), "em step")
 
     def fwd():
-        L.check(lib.lgv_em_forward(h, c["dt"], 0.0, S, c["avg_begin"], c["ckpt"], L.ptr(obs)), "em_forward")
+        L.check(lib.lgv_diff_forward(h, L.MODELA_EM, c["dt"], 0.0, S, c["avg_begin"], c["ckpt"], L.ptr(obs)),
+                "diff_forward")
 
     def bwd():
-        L.check(lib.lgv_em_backward(h, L.ptr(w), L.ptr(g)), "em_backward")
+        L.check(lib.lgv_diff_backward(h, L.ptr(w), L.ptr(g)), "diff_backward")
 
     fwd(), bwd(), plain()  # warm-up (allocations, first launches)
     t_plain, t_fwd, t_bwd = [], [], []

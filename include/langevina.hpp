@@ -570,6 +570,11 @@ class ModelAEulerMaruyama : public LgvStepper {
  public:
   explicit ModelAEulerMaruyama(ModelA &in) : LgvStepper(in, LGV_MODELA_EM) {}
 };
+// Ideal step then Euler-Maruyama relaxation of phi (no counterpart in the reference).
+class IdealEulerMaruyama : public LgvStepper {
+ public:
+  explicit IdealEulerMaruyama(ModelA &in) : LgvStepper(in, LGV_IDEAL_EM) {}
+};
 class PV2HBSplit : public LgvStepper {  // Stepper.h:176-211
  public:
   PV2HBSplit(ModelA &in, const std::array<unsigned int, 2> &scounts = {1, 1}, const bool &nodiffuse = false,
@@ -588,6 +593,7 @@ inline std::unique_ptr<Stepper> make_stepper(ModelA &model, const std::string &e
   if (etype == "PV2HBSplit11") return std::make_unique<PV2HBSplit>(model, std::array<unsigned, 2>{1, 1});
   if (etype == "EulerLangevinHB") return std::make_unique<EulerLangevinHB>(model);
   if (etype == "ModelAEulerMaruyama") return std::make_unique<ModelAEulerMaruyama>(model);
+  if (etype == "IdealEulerMaruyama") return std::make_unique<IdealEulerMaruyama>(model);
   return nullptr;
 }
 

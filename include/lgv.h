@@ -69,6 +69,7 @@ typedef struct lgv_params {
 #define LGV_EULER_LANGEVIN_HB 4      /* B : phi checkerboard heat bath */
 #define LGV_CHARGE_HB 5              /* C : link charge heat bath */
 #define LGV_MODELA_EM 6              /* Euler-Maruyama Model A relaxation */
+#define LGV_IDEAL_EM 7               /* ideal step then Euler-Maruyama relaxation (no counterpart) */
 
 /* Noise sources. */
 #define LGV_NOISE_COUNTER 0  /* counter-indexed xoroshiro128+ streams (production) */
@@ -219,26 +220,33 @@ int lgv_debug_flags(lgv_handle *h, int enable);
 int lgv_get_flags(lgv_handle *h, uint8_t *host_out);
 
 /* ---------------------------------------------------------------------------
- * Differentiable Euler-Maruyama Model A.  No counterpart in the reference (it
- * has no Euler-Maruyama stepper and no gradients); built on the same step as
- * LGV_MODELA_EM.  lgv_em_forward runs S = nsteps steps of size dt from time t
- * with the counter noise (the noise is fixed by seed and counter), keeps a
- * copy of phi every ckpt_every steps and returns two time averages over the
- * steps n = b+1 .. S (b = avg_begin, M = S - b):
+ * Differentiable runs.  No counterpart in the reference (it has no gradients
+ * and no Euler-Maruyama stepper); built on the same steps as lgv_step with
+ * evolver LGV_MODELA_EM (Euler-Maruyama Model A), LGV_IDEAL_PV2 (the ideal
+ * O(4) rotation step) or LGV_IDEAL_EM (both in sequence).  The Metropolis
+ * heat baths have no adjoint.
+ *
+ * lgv_diff_forward runs S = nsteps steps of size dt from time t, the
+ * Euler-Maruyama noise fixed by seed and counter, keeps a copy of the state
+ * every ckpt_every steps and returns two time averages over the steps
+ * n = b+1 .. S (b = avg_begin, M = S - b):
  *   obs[0] = 1/M sum_n sigma(n)                          sigma = <phi_0>
  *   obs[1] = 1/M sum_n V sum_{a=1..3} pibar_a(n)^2      pibar_a = <phi_a>
  * (<.> the volume average, obs[1] the zero-momentum pi equal-time correlator).
- * The lattice is left at the final state and the counter advanced by S.
- * lgv_em_backward returns in grad[4] the derivative of w[0]*obs[0] +
+ * The lattice is left at the final state and the counter advanced by S when
+ * the run has Euler-Maruyama steps (counter noise mode only).
+ * lgv_diff_backward returns in grad[4] the derivative of w[0]*obs[0] +
  * w[1]*obs[1] with respect to (mass0, lambda, H, gamma), the noise held
- * fixed, by the hand-written adjoint of the step; each checkpoint segment is
- * recomputed with the forward's noise.  Counter noise mode only. */
-int lgv_em_forward(lgv_handle *h, double dt, double t, int nsteps, int avg_begin, int ckpt_every, double *obs);
-int lgv_em_backward(lgv_handle *h, const double *w, double *grad);
-/* The volume averages <phi_a>(n), n = 0..nsteps, a = 0..3, of the last
- * lgv_em_forward (out holds (nsteps+1)*4 doubles; nsteps must be the
- * forward's). */
-int lgv_em_averages(lgv_handle *h, double *out, int nsteps);
+ * fixed, by the hand-written adjoint kernels of the steps; each checkpoint
+ * segment is recomputed with the forward's noise.  It may be called any
+ * number of times after one forward.
+ * lgv_diff_averages copies the volume averages <phi_a>(n), n = 0..nsteps,
+ * a = 0..3, of the last forward into out ((nsteps+1)*4 doubles; nsteps must
+ * be the forward's). */
+int lgv_diff_forward(lgv_handle *h, int evolver, double dt, double t, int nsteps, int avg_begin, int ckpt_every,
+                     double *obs);
+int lgv_diff_backward(lgv_handle *h, const double *w, double *grad);
+int lgv_diff_averages(lgv_handle *h, double *out, int nsteps);
 
 /* ---------------------------------------------------------------------------
  * Batched ensembles.  Replaces running an ensemble as separate processes or

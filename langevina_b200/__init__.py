@@ -5,7 +5,7 @@ host mirror.  Importing it loads the library and raises if it is missing.
 """
 from . import _lib
 from ._lib import LgvError, Measurement, load, make_params  # noqa: F401
-from .model import (EulerLangevinHB, IdealPV2, Measurer, ModelA, ModelAData,  # noqa: F401
+from .model import (EulerLangevinHB, IdealEulerMaruyama, IdealPV2, Measurer, ModelA, ModelAData,  # noqa: F401
                     ModelAEulerMaruyama, ModelGChargeHB, PV2HBSplit, Stepper, make_stepper)
 
 lib = load()

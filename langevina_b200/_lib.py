@@ -17,7 +17,7 @@ NOBS, NOBS_PHASE = 11, 14
 NOALLOC_MAX_N = 128
 
 PV2HBSPLIT, PV2HBSPLIT_NODIFFUSE, PV2HBSPLIT_ONLYDIFFUSE = 0, 1, 2
-IDEAL_PV2, EULER_LANGEVIN_HB, CHARGE_HB, MODELA_EM = 3, 4, 5, 6
+IDEAL_PV2, EULER_LANGEVIN_HB, CHARGE_HB, MODELA_EM, IDEAL_EM = 3, 4, 5, 6, 7
 NOISE_COUNTER, NOISE_INJECTED = 0, 1
 INIT_ZERO, INIT_PHI_GAUSSIAN, INIT_CHARGES_GAUSSIAN = 0, 1, 2
 MONITOR_IDEAL, MONITOR_PHI_HB, MONITOR_CHARGE_HB = 0, 1, 2
@@ -82,9 +82,9 @@ SIGNATURES = [
     ("lgv_debug_flags", C.c_int, [_H, C.c_int]),
     ("lgv_get_flags", C.c_int, [_H, C.c_void_p]),
     ("lgv_measure_aos_noalloc", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
-    ("lgv_em_forward", C.c_int, [_H, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, C.c_void_p]),
-    ("lgv_em_backward", C.c_int, [_H, C.c_void_p, C.c_void_p]),
-    ("lgv_em_averages", C.c_int, [_H, C.c_void_p, C.c_int]),
+    ("lgv_diff_forward", C.c_int, [_H, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, C.c_void_p]),
+    ("lgv_diff_backward", C.c_int, [_H, C.c_void_p, C.c_void_p]),
+    ("lgv_diff_averages", C.c_int, [_H, C.c_void_p, C.c_int]),
     ("lgv_ensemble_create", C.c_int, [C.c_int, C.c_void_p, C.POINTER(_H)]),
     ("lgv_ensemble_destroy", C.c_int, [_H]),
     ("lgv_ensemble_size", C.c_int, [_H, C.POINTER(C.c_int)]),

@@ -105,17 +105,20 @@ struct lgv_handle {
   double t_ms[LGV_NKCLASS] = {0};
   int64_t t_n[LGV_NKCLASS] = {0};
   // differentiable Euler-Maruyama run (lgv_em_forward / lgv_em_backward)
+  // differentiable run (lgv_diff_forward / lgv_diff_backward)
   struct {
     bool ready = false;
-    lgv_params p{};  // parameters and key of the forward run, used by the backward
+    int ev = 0, ncomp = 4;  // evolver; planes per stored state (phi only, or phi and charges)
+    lgv_params p{};         // parameters and key of the forward run, used by the backward
     uint64_t key = 0;
     double dt = 0;
     int S = 0, b = 0, K = 1;
     uint64_t ctr0 = 0;
     std::vector<double> tn, avg;
-    double *ckpt = nullptr, *seg = nullptr, *lam = nullptr, *avg_dev = nullptr, *partial = nullptr, *g4 = nullptr;
+    double *ckpt = nullptr, *seg = nullptr, *lam = nullptr, *work = nullptr, *avg_dev = nullptr, *partial = nullptr,
+           *g4 = nullptr;
     unsigned *done = nullptr;  // grid_sum4 counter, zero between launches
-    size_t ckpt_len = 0, seg_len = 0, avg_len = 0, lam_len = 0;
+    size_t ckpt_len = 0, seg_len = 0, avg_len = 0, lam_len = 0, work_len = 0;
   } adj;
 };
 
@@ -366,6 +369,9 @@ int step_once(lgv_handle *h, int ev, int inner, int outer, double dt, double t) 
     case LGV_EULER_LANGEVIN_HB: return sub_hb(h, dt, mass);
     case LGV_CHARGE_HB: return sub_charge(h, dt);
     case LGV_MODELA_EM: return sub_em(h, dt, mass);
+    case LGV_IDEAL_EM:
+      LGV_TRY(sub_ideal(h, dt));
+      return sub_em(h, dt, mass);
     default: return fail(LGV_ERR_INVALID, "unknown evolver %d", ev);
   }
 }
@@ -457,7 +463,7 @@ int lgv_destroy(lgv_handle *h) {
     if (b) cudaFree(b);
   if (h->mon_dev) cudaFree(h->mon_dev);
   if (h->flags_dev) cudaFree(h->flags_dev);
-  for (double *b : {h->adj.ckpt, h->adj.seg, h->adj.lam, h->adj.avg_dev, h->adj.partial, h->adj.g4})
+  for (double *b : {h->adj.ckpt, h->adj.seg, h->adj.lam, h->adj.work, h->adj.avg_dev, h->adj.partial, h->adj.g4})
     if (b) cudaFree(b);
   if (h->adj.done) cudaFree(h->adj.done);
   for (auto &u : h->ev_used) {
@@ -734,7 +740,8 @@ int lgv_timing_read(lgv_handle *h, int kclass, double *total_ms, int64_t *launch
 }
 
 // ---------------------------------------------------------------------------
-// Differentiable Euler-Maruyama Model A run.
+// Differentiable runs: Euler-Maruyama Model A, the ideal step, or the two in
+// sequence, with the noise fixed by seed and counter.
 namespace {
 
 int adj_realloc(double **p, size_t *len, size_t n) {
@@ -747,9 +754,10 @@ int adj_realloc(double **p, size_t *len, size_t n) {
   return LGV_OK;
 }
 
-Fields phi_slot(double *base, size_t V, size_t slot) {
+// planes first .. first+n-1 of a buffer of V-double planes as Fields c[0..n-1]
+Fields planes(double *base, size_t V, size_t first, int n) {
   Fields f{};
-  for (int l = 0; l < 4; ++l) f.c[l] = base + (slot * 4 + l) * V;
+  for (int l = 0; l < n; ++l) f.c[l] = base + (first + l) * V;
   return f;
 }
 
@@ -778,20 +786,41 @@ lgv::EmArgs em_args(const lgv_params &p, uint64_t key, uint64_t ctr, double dt, 
   return e;
 }
 
+// arguments of an ideal step of size dt, as sub_ideal builds them
+lgv::IdealArgs ideal_args(const lgv_params &p, int N, double dt) {
+  lgv::IdealArgs a{};
+  a.dto2chi = (dt / 2.0) / p.chi;
+  a.dt = dt;
+  const double hx = p.LX / N;
+  a.a2 = std::pow(1.0 / hx, 2);
+  a.H = p.H;
+  return a;
+}
+
+bool has_ideal(int ev) { return ev == LGV_IDEAL_PV2 || ev == LGV_IDEAL_EM; }
+bool has_em(int ev) { return ev == LGV_MODELA_EM || ev == LGV_IDEAL_EM; }
+
 }  // namespace
 
-int lgv_em_forward(lgv_handle *h, double dt, double t, int nsteps, int avg_begin, int ckpt_every, double *obs) {
+int lgv_diff_forward(lgv_handle *h, int evolver, double dt, double t, int nsteps, int avg_begin, int ckpt_every,
+                     double *obs) {
   if (!h || !obs) return fail(LGV_ERR_INVALID, "NULL argument");
+  if (!has_ideal(evolver) && !has_em(evolver))
+    return fail(LGV_ERR_INVALID, "lgv_diff_forward: evolver %d has no adjoint (LGV_MODELA_EM, LGV_IDEAL_PV2, LGV_IDEAL_EM)",
+                evolver);
   if (nsteps < 1 || avg_begin < 0 || avg_begin >= nsteps || ckpt_every < 1)
-    return fail(LGV_ERR_INVALID, "lgv_em_forward: need nsteps >= 1, 0 <= avg_begin < nsteps, ckpt_every >= 1");
-  if (h->noise_mode != LGV_NOISE_COUNTER) return fail(LGV_ERR_STATE, "lgv_em_forward needs counter noise");
+    return fail(LGV_ERR_INVALID, "lgv_diff_forward: need nsteps >= 1, 0 <= avg_begin < nsteps, ckpt_every >= 1");
+  if (has_em(evolver) && h->noise_mode != LGV_NOISE_COUNTER)
+    return fail(LGV_ERR_STATE, "lgv_diff_forward needs counter noise");
   DeviceGuard g(h->device);
   auto &A = h->adj;
   A.ready = false;
   const size_t V = h->V;
   const int S = nsteps, K = ckpt_every;
+  A.ev = evolver;
+  A.ncomp = has_ideal(evolver) ? 10 : 4;
   const size_t nck = (size_t)(S - 1) / K + 1;
-  LGV_TRY(adj_realloc(&A.ckpt, &A.ckpt_len, nck * 4 * V));
+  LGV_TRY(adj_realloc(&A.ckpt, &A.ckpt_len, nck * A.ncomp * V));
   LGV_TRY(adj_realloc(&A.avg_dev, &A.avg_len, (size_t)(S + 1) * 4));
   LGV_TRY(adj_counters(h));
   A.dt = dt;
@@ -804,21 +833,29 @@ int lgv_em_forward(lgv_handle *h, double dt, double t, int nsteps, int avg_begin
   A.tn.assign(S + 1, 0.0);
   A.tn[0] = t;
   for (int n = 0; n < S; ++n) A.tn[n + 1] = A.tn[n] + dt;
+  const lgv::IdealArgs ia = ideal_args(A.p, h->N, dt);
   LGV_CK(lgv::launch_phi_avg(h->cur, h->N, A.partial, A.done, A.avg_dev, h->stream));
-  {
-    KTimer tm(h, LGV_KCLASS_EM);
-    for (int n = 0; n < S; ++n) {
-      if (n % K == 0)
-        for (int l = 0; l < 4; ++l)
-          LGV_CK(cudaMemcpyAsync(A.ckpt + ((size_t)(n / K) * 4 + l) * V, h->cur.c[l], V * sizeof(double),
-                                 cudaMemcpyDeviceToDevice, h->stream));
+  for (int n = 0; n < S; ++n) {
+    if (n % K == 0)
+      for (int l = 0; l < A.ncomp; ++l)
+        LGV_CK(cudaMemcpyAsync(A.ckpt + ((size_t)(n / K) * A.ncomp + l) * V, h->cur.c[l], V * sizeof(double),
+                               cudaMemcpyDeviceToDevice, h->stream));
+    double *avg_n = A.avg_dev + (size_t)(n + 1) * 4;
+    if (has_ideal(evolver)) {
+      KTimer tm(h, LGV_KCLASS_IDEAL);
+      LGV_CK(lgv::launch_ideal(h->cur, h->alt, h->N, ia, h->stream));
+      std::swap(h->cur, h->alt);
+    }
+    if (has_em(evolver)) {
+      KTimer tm(h, LGV_KCLASS_EM);
       const lgv::EmArgs e = em_args(A.p, A.key, A.ctr0 + (uint64_t)n, dt, A.tn[n]);
-      LGV_CK(lgv::launch_em_avg(h->cur, h->alt, h->N, e, A.partial, A.done, A.avg_dev + (size_t)(n + 1) * 4,
-                                h->stream));
+      LGV_CK(lgv::launch_em_avg(h->cur, h->alt, h->N, e, A.partial, A.done, avg_n, h->stream));
       for (int l = 0; l < 4; ++l) std::swap(h->cur.c[l], h->alt.c[l]);
+    } else {
+      LGV_CK(lgv::launch_phi_avg(h->cur, h->N, A.partial, A.done, avg_n, h->stream));
     }
   }
-  h->ctr += (uint64_t)S;
+  if (has_em(evolver)) h->ctr += (uint64_t)S;
   A.avg.assign((size_t)(S + 1) * 4, 0.0);
   LGV_CK(cudaMemcpyAsync(A.avg.data(), A.avg_dev, A.avg.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   LGV_CK(cudaStreamSynchronize(h->stream));
@@ -837,23 +874,26 @@ int lgv_em_forward(lgv_handle *h, double dt, double t, int nsteps, int avg_begin
   return LGV_OK;
 }
 
-int lgv_em_averages(lgv_handle *h, double *out, int nsteps) {
+int lgv_diff_averages(lgv_handle *h, double *out, int nsteps) {
   if (!h || !out) return fail(LGV_ERR_INVALID, "NULL argument");
-  if (!h->adj.ready) return fail(LGV_ERR_STATE, "lgv_em_averages: no forward run");
-  if (nsteps != h->adj.S) return fail(LGV_ERR_INVALID, "lgv_em_averages: nsteps %d != forward's %d", nsteps, h->adj.S);
+  if (!h->adj.ready) return fail(LGV_ERR_STATE, "lgv_diff_averages: no forward run");
+  if (nsteps != h->adj.S)
+    return fail(LGV_ERR_INVALID, "lgv_diff_averages: nsteps %d != forward's %d", nsteps, h->adj.S);
   std::copy(h->adj.avg.begin(), h->adj.avg.end(), out);
   return LGV_OK;
 }
 
-int lgv_em_backward(lgv_handle *h, const double *w, double *grad) {
+int lgv_diff_backward(lgv_handle *h, const double *w, double *grad) {
   if (!h || !w || !grad) return fail(LGV_ERR_INVALID, "NULL argument");
   auto &A = h->adj;
-  if (!A.ready) return fail(LGV_ERR_STATE, "lgv_em_backward: no forward run to differentiate");
+  if (!A.ready) return fail(LGV_ERR_STATE, "lgv_diff_backward: no forward run to differentiate");
   DeviceGuard g(h->device);
   const size_t V = h->V;
-  const int S = A.S, K = A.K, M = S - A.b;
-  LGV_TRY(adj_realloc(&A.seg, &A.seg_len, (size_t)K * 4 * V));
-  LGV_TRY(adj_realloc(&A.lam, &A.lam_len, 2 * 4 * V));
+  const int S = A.S, K = A.K, M = S - A.b, nc = A.ncomp, N = h->N;
+  const int ev = A.ev;
+  LGV_TRY(adj_realloc(&A.seg, &A.seg_len, (size_t)K * nc * V));
+  LGV_TRY(adj_realloc(&A.lam, &A.lam_len, 2 * 10 * V));
+  if (has_ideal(ev)) LGV_TRY(adj_realloc(&A.work, &A.work_len, 28 * V));
   LGV_TRY(adj_counters(h));
   LGV_CK(cudaMemsetAsync(A.g4, 0, 4 * sizeof(double), h->stream));
   const double Vd = (double)V;
@@ -865,38 +905,78 @@ int lgv_em_backward(lgv_handle *h, const double *w, double *grad) {
     out[0] = w[0] / (Vd * M);
     for (int a = 1; a < 4; ++a) out[a] = w[1] * 2.0 * av[a] / M;
   };
+  const lgv::IdealArgs ia = ideal_args(A.p, N, A.dt);
+  lgv::IdealAdjArgs iadj{};
+  iadj.k = ia.dto2chi;
+  iadj.dt = ia.dt;
+  iadj.a2 = ia.a2;
+  iadj.H = ia.H;
+  // work planes: tmp state (0..9), phi adjoint after the EM step (10..13), P1 (14..17), PB (18..21), QB (22..27)
+  const Fields tmp = planes(A.work, V, 0, 10), lamx = planes(A.work, V, 10, 4), P1 = planes(A.work, V, 14, 4),
+               PB = planes(A.work, V, 18, 4), QB = planes(A.work, V, 22, 6);
+  auto lam = [&](int which) { return planes(A.lam, V, (size_t)which * 10, 10); };
+  auto slot = [&](int m) { return planes(A.seg, V, (size_t)m * nc, nc); };
   int cur = 0;
   {
     double v[4];
     gl(S, v);
-    LGV_CK(lgv::launch_fill_phi(phi_slot(A.lam, V, 0), h->N, v, h->stream));
+    LGV_CK(cudaMemsetAsync(A.lam, 0, 10 * V * sizeof(double), h->stream));
+    LGV_CK(lgv::launch_fill_phi(lam(0), N, v, h->stream));
   }
   int loaded = -1;
   for (int n = S - 1; n >= 0; --n) {
     const int s = n / K;
     if (s != loaded) {
-      // phi_{sK} .. phi_{min(sK+K, S)-1} again from the checkpoint, with the forward's noise
-      for (int l = 0; l < 4; ++l)
-        LGV_CK(cudaMemcpyAsync(A.seg + (size_t)l * V, A.ckpt + ((size_t)s * 4 + l) * V, V * sizeof(double),
+      // states u_{sK} .. u_{min(sK+K, S)-1} again from the checkpoint, with the forward's noise
+      for (int l = 0; l < nc; ++l)
+        LGV_CK(cudaMemcpyAsync(A.seg + (size_t)l * V, A.ckpt + ((size_t)s * nc + l) * V, V * sizeof(double),
                                cudaMemcpyDeviceToDevice, h->stream));
       const int last = std::min(s * K + K - 1, S - 1);
       for (int m = s * K; m < last; ++m) {
+        const Fields a = slot(m - s * K), b = slot(m - s * K + 1);
         const lgv::EmArgs e = em_args(A.p, A.key, A.ctr0 + (uint64_t)m, A.dt, A.tn[m]);
-        LGV_CK(lgv::launch_em(phi_slot(A.seg, V, m - s * K), phi_slot(A.seg, V, m - s * K + 1), h->N, e, h->stream));
+        if (ev == LGV_MODELA_EM) {
+          LGV_CK(lgv::launch_em(a, b, N, e, h->stream));
+        } else if (ev == LGV_IDEAL_PV2) {
+          LGV_CK(lgv::launch_ideal(a, b, N, ia, h->stream));
+        } else {
+          Fields mid = b;  // phi to tmp, charges straight into the next slot
+          for (int l = 0; l < 4; ++l) mid.c[l] = tmp.c[l];
+          LGV_CK(lgv::launch_ideal(a, mid, N, ia, h->stream));
+          LGV_CK(lgv::launch_em(mid, b, N, e, h->stream));
+        }
       }
       loaded = s;
     }
-    lgv::EmAdjArgs a{};
-    a.c6 = 6.0 + (A.p.mass0 + A.p.dmassdt * A.tn[n]);
-    a.dtg = A.dt * A.p.gamma;
-    a.dt = A.dt;
-    a.lambda = A.p.lambda;
-    a.H = A.p.H;
-    a.cxi = std::sqrt(2.0 * A.dt) / (2.0 * std::sqrt(A.p.gamma));
-    gl(n, a.gl);
-    a.sk = lgv::sub_key(A.key, A.ctr0 + (uint64_t)n);
-    LGV_CK(lgv::launch_em_adjoint(phi_slot(A.seg, V, n - s * K), phi_slot(A.lam, V, cur), phi_slot(A.lam, V, cur ^ 1),
-                                  h->N, a, A.partial, A.done, A.g4, h->stream));
+    const Fields u = slot(n - s * K);
+    double gln[4];
+    gl(n, gln);
+    if (has_em(ev)) {
+      lgv::EmAdjArgs a{};
+      a.c6 = 6.0 + (A.p.mass0 + A.p.dmassdt * A.tn[n]);
+      a.dtg = A.dt * A.p.gamma;
+      a.dt = A.dt;
+      a.lambda = A.p.lambda;
+      a.H = A.p.H;
+      a.cxi = std::sqrt(2.0 * A.dt) / (2.0 * std::sqrt(A.p.gamma));
+      a.sk = lgv::sub_key(A.key, A.ctr0 + (uint64_t)n);
+      if (ev == LGV_MODELA_EM) {
+        for (int q = 0; q < 4; ++q) a.gl[q] = gln[q];
+        LGV_CK(lgv::launch_em_adjoint(u, lam(cur), lam(cur ^ 1), N, a, A.partial, A.done, A.g4, h->stream));
+      } else {
+        LGV_CK(lgv::launch_ideal(u, tmp, N, ia, h->stream));
+        LGV_CK(lgv::launch_em_adjoint(tmp, lam(cur), lamx, N, a, A.partial, A.done, A.g4, h->stream));
+        Fields lmid = lam(cur);  // charges' adjoint passes the EM step unchanged
+        for (int l = 0; l < 4; ++l) lmid.c[l] = lamx.c[l];
+        for (int q = 0; q < 4; ++q) iadj.gl[q] = gln[q];
+        LGV_CK(lgv::launch_ideal_adjoint(u, lmid, lam(cur ^ 1), P1, PB, QB, N, iadj, A.partial, A.done, A.g4,
+                                         h->stream));
+      }
+    } else {
+      for (int q = 0; q < 4; ++q) iadj.gl[q] = gln[q];
+      LGV_CK(lgv::launch_ideal_adjoint(u, lam(cur), lam(cur ^ 1), P1, PB, QB, N, iadj, A.partial, A.done, A.g4,
+                                       h->stream));
+    }
     cur ^= 1;
   }
   LGV_CK(cudaMemcpyAsync(grad, A.g4, 4 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));

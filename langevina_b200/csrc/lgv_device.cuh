@@ -174,4 +174,88 @@ __device__ __forceinline__ void rotate_site(double phi[4], const double q[6], do
   o4_rotate(muV, muA, phi);
 }
 
+// ---------------------------------------------------------------------------
+// Adjoint of the O(4) rotation (no counterpart in the reference).
+//
+// expmul_d: w = expmul(v) and, for its adjoint, sc = sin|v|/|v| and
+// ds = d sc / d|v|^2, the latter from the Maclaurin series
+// sum_{n>=1} (-1)^n n x^(2n-2) / (2n+1)! for |v|^2 <= 1/16 (8 terms; the next
+// is below 1e-22 relative) and (cos|v| - sc) / (2|v|^2) beyond.
+__device__ __forceinline__ void expmul_d(const double v[3], double w[4], double &sc, double &ds) {
+  const double x2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+  double c;
+  cos_sinc(x2, c, sc);
+  if (x2 <= 0.0625) {
+    ds = 1.0 / 44460928512000.0;        //  8 / 17!
+    ds = fma(ds, x2, -1.0 / 186810624000.0);  // -7 / 15!
+    ds = fma(ds, x2, 1.0 / 1037836800.0);     //  6 / 13!
+    ds = fma(ds, x2, -1.0 / 7983360.0);       // -5 / 11!
+    ds = fma(ds, x2, 1.0 / 90720.0);          //  4 / 9!
+    ds = fma(ds, x2, -1.0 / 1680.0);          // -3 / 7!
+    ds = fma(ds, x2, 1.0 / 60.0);             //  2 / 5!
+    ds = fma(ds, x2, -1.0 / 6.0);             // -1 / 3!
+  } else {
+    ds = (c - sc) / (2.0 * x2);
+  }
+  if (x2 > 1e-40) {  // the forward's identity below |v| = 1e-20
+    w[0] = c;
+    w[1] = -sc * v[0];
+    w[2] = -sc * v[1];
+    w[3] = -sc * v[2];
+  } else {
+    w[0] = 1.0;
+    w[1] = w[2] = w[3] = 0.0;
+  }
+}
+
+// v_bar of w = expmul(v) given w_bar: dw0/dv = -sc v, dw_j/dv_i = -sc d_ij - 2 ds v_i v_j.
+__device__ __forceinline__ void expmul_adj(const double v[3], double sc, double ds, const double wb[4], double vb[3]) {
+  const double vd = wb[1] * v[0] + wb[2] * v[1] + wb[3] * v[2];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) vb[i] = -sc * (wb[0] * v[i] + wb[1 + i]) - 2.0 * ds * v[i] * vd;
+}
+
+__device__ __forceinline__ void qconj(const double a[4], double w[4]) {
+  w[0] = a[0];
+  w[1] = -a[1];
+  w[2] = -a[2];
+  w[3] = -a[3];
+}
+
+// Adjoint of out = rotate_site(phi, q, k): given ob = d/d out, returns
+// pb = d/d phi and qb = d/d q.  Quaternion products are bilinear with
+// transposes given by the conjugate: for w = a b, a_bar = w_bar conj(b) and
+// b_bar = conj(a) w_bar.
+__device__ __forceinline__ void rotate_site_adj(const double phi[4], const double q[6], double k, const double ob[4],
+                                                double pb[4], double qb[6]) {
+  double vR[3], vL[3];
+#pragma unroll
+  for (int s = 0; s < 3; ++s) {
+    const double muA = -q[s] * k, muV = -q[3 + s] * k;
+    vR[s] = -0.5 * (muV - muA);
+    vL[s] = 0.5 * (muV + muA);
+  }
+  double R[4], L[4], scR, dsR, scL, dsL;
+  expmul_d(vR, R, scR, dsR);
+  expmul_d(vL, L, scL, dsL);
+  double t[4], cj[4], tb[4], Lb[4], Rb[4];
+  quatmul(phi, R, t);
+  qconj(L, cj);
+  quatmul(cj, ob, tb);
+  qconj(t, cj);
+  quatmul(ob, cj, Lb);
+  qconj(R, cj);
+  quatmul(tb, cj, pb);
+  qconj(phi, cj);
+  quatmul(cj, tb, Rb);
+  double vLb[3], vRb[3];
+  expmul_adj(vL, scL, dsL, Lb, vLb);
+  expmul_adj(vR, scR, dsR, Rb, vRb);
+#pragma unroll
+  for (int s = 0; s < 3; ++s) {
+    qb[s] = -k * (0.5 * vLb[s] + 0.5 * vRb[s]);      // via mu_A
+    qb[3 + s] = -k * (0.5 * vLb[s] - 0.5 * vRb[s]);  // via mu_V
+  }
+}
+
 }  // namespace lgv

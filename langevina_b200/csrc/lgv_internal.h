@@ -120,6 +120,21 @@ struct EmAdjArgs {
 };
 // lam_out = J^T lam_in + gl at state phi; per-block parameter-gradient partial
 // sums (dm2, dlambda, dH, dgamma) into partial[nblocks][4]
+struct IdealAdjArgs {
+  double k;   // (dt / 2) / chi
+  double dt;
+  double a2;  // (1 / h)^2
+  double H;
+  double gl[4];  // added to the phi adjoint at every site
+};
+
+// Adjoint of one ideal step at state u (10 planes): lam_in (10 planes) ->
+// lam_out (10 planes); adds dL/dH into g4[2].  P1, PB: 4 planes, QB: 6 planes
+// of scratch; partial / done as for launch_em_avg.
+cudaError_t launch_ideal_adjoint(Fields u, Fields lam_in, Fields lam_out, Fields P1, Fields PB, Fields QB, int N,
+                                 const IdealAdjArgs &a, double *partial, unsigned *done, double *g4,
+                                 cudaStream_t st);
+
 // Euler-Maruyama step that also writes the volume averages of the new phi
 // to avg_out[0..3]; partial holds em_reduce_blocks(N) * 4 doubles and *done
 // is a zeroed counter (left zeroed).

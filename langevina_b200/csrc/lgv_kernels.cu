@@ -1527,6 +1527,167 @@ __global__ void __launch_bounds__(kAdjThreads, 4) em_adjoint_kernel(Fields phi, 
   grid_sum4<kAdjThreads>(v, partial, done, g4, 1.0, true);
 }
 
+// ----------------------------------------------------------------------------
+// Adjoint of the ideal step (IdealPV2::step_no_reject, Stepper.cxx:68-176):
+//   phi1 = rot(phi, n), n' = n + dt J(phi1), phi2 = rot(phi1, n'),
+// with the currents J, summed over directions,
+//   J_A,l = a2 (phi1_0 S_l - phi1_l S_0) - H phi1_l,
+//   J_V,s = a2 (phi1_s1 S_s2 - phi1_s2 S_s1),   S_a = sum_nbr phi1_a.
+// Three passes: rot_phi_kernel writes phi1; ideal_adj_a_kernel recomputes n'
+// exactly as the forward does and back-propagates through the second
+// rotation (phi1_bar partial -> PB, n'_bar -> QB, dL/dH); ideal_adj_b_kernel
+// adds the currents' adjoint (a stencil over QB * phi1), back-propagates
+// through the first rotation and writes lam_out = (phi_bar + gl, n_bar).
+// Pair (a, b, c): charge c gets a2 (phi1_a S_b - phi1_b S_a).
+__host__ __device__ constexpr int pair_a(int c) { return c < 3 ? 0 : (c == 3 ? 2 : (c == 4 ? 3 : 1)); }
+__host__ __device__ constexpr int pair_b(int c) { return c < 3 ? c + 1 : (c == 3 ? 3 : (c == 4 ? 1 : 2)); }
+
+struct SiteNbrs {
+  long long own, o[6];  // x+, x-, y+, y-, z+, z-
+};
+
+__device__ __forceinline__ SiteNbrs site_nbrs(const Geo &g, int m, int j, int k, int parity) {
+  const int H = g.H, N = g.N;
+  const long long row = ((long long)k * N + j) * H;
+  const int s = (parity + j + k) & 1;
+  int xm = m - 1 + s, xp = m + s;
+  if (xm < 0) xm += H;
+  if (xp == H) xp = 0;
+  const long long ob = (long long)(parity ^ 1) * g.V2;
+  SiteNbrs r;
+  r.own = (long long)parity * g.V2 + row + m;
+  r.o[0] = ob + row + xp;
+  r.o[1] = ob + row + xm;
+  r.o[2] = ob + ((long long)k * N + wrap_inc(j, N)) * H + m;
+  r.o[3] = ob + ((long long)k * N + wrap_dec(j, N)) * H + m;
+  r.o[4] = ob + ((long long)wrap_inc(k, N) * N + j) * H + m;
+  r.o[5] = ob + ((long long)wrap_dec(k, N) * N + j) * H + m;
+  return r;
+}
+
+__global__ void __launch_bounds__(kThreads) rot_phi_kernel(Fields u, Fields P1, long long V, double k) {
+  const long long n = (long long)blockIdx.x * kThreads + threadIdx.x;
+  if (n >= V) return;
+  double ph[4], q[6];
+#pragma unroll
+  for (int l = 0; l < 4; ++l) ph[l] = u.c[l][n];
+#pragma unroll
+  for (int s = 0; s < 6; ++s) q[s] = u.c[4 + s][n];
+  rotate_site(ph, q, k);
+#pragma unroll
+  for (int l = 0; l < 4; ++l) P1.c[l][n] = ph[l];
+}
+
+__global__ void __launch_bounds__(128) ideal_adj_a_kernel(Fields u, Fields lin, Fields P1, Fields PB, Fields QB, Geo g,
+                                                          IdealAdjArgs a, double *partial, unsigned *done,
+                                                          double *g4) {
+  const long long idx = (long long)blockIdx.x * 128 + threadIdx.x;
+  double hb = 0;
+  if (idx < g.V2) {
+    int m, j, k;
+    pair_coords(idx, g, m, j, k);
+#pragma unroll 1
+    for (int parity = 0; parity < 2; ++parity) {
+      const SiteNbrs sn = site_nbrs(g, m, j, k, parity);
+      double c[4], xp[4], xm[4], yp[4], ym[4], zp[4], zm[4];
+#pragma unroll
+      for (int l = 0; l < 4; ++l) {
+        const double *P = P1.c[l];
+        c[l] = P[sn.own];
+        xp[l] = P[sn.o[0]];
+        xm[l] = P[sn.o[1]];
+        yp[l] = P[sn.o[2]];
+        ym[l] = P[sn.o[3]];
+        zp[l] = P[sn.o[4]];
+        zm[l] = P[sn.o[5]];
+      }
+      double q2[6];
+      // n' exactly as the forward computes it (ideal_tile)
+#pragma unroll
+      for (int l = 0; l < 3; ++l) {
+        const double bx = -xp[0] * c[l + 1] + c[0] * xp[l + 1] + c[0] * xm[l + 1] - xm[0] * c[l + 1];
+        const double by = -yp[0] * c[l + 1] + c[0] * yp[l + 1] + c[0] * ym[l + 1] - ym[0] * c[l + 1];
+        const double bz = -zp[0] * c[l + 1] + c[0] * zp[l + 1] + c[0] * zm[l + 1] - zm[0] * c[l + 1];
+        q2[l] = u.c[4 + l][sn.own] + a.dt * (bx * a.a2 + by * a.a2 + bz * a.a2 - a.H * c[l + 1]);
+      }
+#pragma unroll
+      for (int s = 0; s < 3; ++s) {
+        const int s1 = 1 + (s + 1) % 3, s2 = 1 + (s + 2) % 3;
+        const double bx = xp[s2] * c[s1] - c[s2] * xm[s1] - xp[s1] * c[s2] + c[s1] * xm[s2];
+        const double by = yp[s2] * c[s1] - c[s2] * ym[s1] - yp[s1] * c[s2] + c[s1] * ym[s2];
+        const double bz = zp[s2] * c[s1] - c[s2] * zm[s1] - zp[s1] * c[s2] + c[s1] * zm[s2];
+        q2[3 + s] = u.c[7 + s][sn.own] + a.dt * (bx * a.a2 + by * a.a2 + bz * a.a2);
+      }
+      double ob[4], pb[4], qb[6];
+#pragma unroll
+      for (int l = 0; l < 4; ++l) ob[l] = lin.c[l][sn.own];
+      rotate_site_adj(c, q2, a.k, ob, pb, qb);
+#pragma unroll
+      for (int l = 0; l < 4; ++l) PB.c[l][sn.own] = pb[l];
+#pragma unroll
+      for (int s = 0; s < 6; ++s) {
+        const double Q = lin.c[4 + s][sn.own] + qb[s];
+        QB.c[s][sn.own] = Q;
+        if (s < 3) hb += -a.dt * Q * c[s + 1];
+      }
+    }
+  }
+  double v[4] = {0.0, 0.0, hb, 0.0};
+  grid_sum4<128>(v, partial, done, g4, 1.0, true);
+}
+
+__global__ void __launch_bounds__(128) ideal_adj_b_kernel(Fields u, Fields lout, Fields P1, Fields PB, Fields QB, Geo g,
+                                                          IdealAdjArgs a) {
+  const long long idx = (long long)blockIdx.x * 128 + threadIdx.x;
+  if (idx >= g.V2) return;
+  int m, j, k;
+  pair_coords(idx, g, m, j, k);
+#pragma unroll 1
+  for (int parity = 0; parity < 2; ++parity) {
+    const SiteNbrs sn = site_nbrs(g, m, j, k, parity);
+    double S[4] = {0, 0, 0, 0}, Na[6] = {0, 0, 0, 0, 0, 0}, Nb[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int d = 0; d < 6; ++d) {
+      double P[4], Q[6];
+#pragma unroll
+      for (int l = 0; l < 4; ++l) P[l] = P1.c[l][sn.o[d]];
+#pragma unroll
+      for (int s = 0; s < 6; ++s) Q[s] = QB.c[s][sn.o[d]];
+#pragma unroll
+      for (int l = 0; l < 4; ++l) S[l] += P[l];
+#pragma unroll
+      for (int c = 0; c < 6; ++c) {
+        Na[c] += Q[c] * P[pair_b(c)];
+        Nb[c] += Q[c] * P[pair_a(c)];
+      }
+    }
+    double pb[4], Qc[6];
+#pragma unroll
+    for (int l = 0; l < 4; ++l) pb[l] = PB.c[l][sn.own];
+#pragma unroll
+    for (int s = 0; s < 6; ++s) Qc[s] = QB.c[s][sn.own];
+    const double da = a.dt * a.a2;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+      const int ia = pair_a(c), ib = pair_b(c);
+      pb[ia] += da * (Qc[c] * S[ib] - Na[c]);
+      pb[ib] += da * (Nb[c] - Qc[c] * S[ia]);
+    }
+#pragma unroll
+    for (int l = 0; l < 3; ++l) pb[l + 1] += -a.dt * a.H * Qc[l];
+    double ph[4], q[6], phb[4], qb[6];
+#pragma unroll
+    for (int l = 0; l < 4; ++l) ph[l] = u.c[l][sn.own];
+#pragma unroll
+    for (int s = 0; s < 6; ++s) q[s] = u.c[4 + s][sn.own];
+    rotate_site_adj(ph, q, a.k, pb, phb, qb);
+#pragma unroll
+    for (int l = 0; l < 4; ++l) lout.c[l][sn.own] = phb[l] + a.gl[l];
+#pragma unroll
+    for (int s = 0; s < 6; ++s) lout.c[4 + s][sn.own] = Qc[s] + qb[s];
+  }
+}
+
 // volume averages of phi_0..3 into out[0..3]
 __global__ void __launch_bounds__(kThreads) phi_avg_kernel(Fields f, Geo g, double *partial, unsigned *done,
                                                            double *out) {
@@ -1883,7 +2044,7 @@ cudaError_t launch_batch_oavg_final(const RepDesc *d, const int *first, const in
 // Euler-Maruyama adjoint launchers.
 size_t em_reduce_blocks(int N) {
   const Geo g = make_geo(N);
-  return std::max<size_t>(nblocks(g.V2, kThreads), nblocks(g.V2, kAdjThreads));
+  return std::max<size_t>(nblocks(g.V2, kThreads), nblocks(g.V2, std::min(kAdjThreads, 128)));
 }
 
 cudaError_t launch_em_adjoint(Fields phi, Fields lam_in, Fields lam_out, int N, const EmAdjArgs &a, double *partial,
@@ -1891,6 +2052,17 @@ cudaError_t launch_em_adjoint(Fields phi, Fields lam_in, Fields lam_out, int N, 
   const Geo g = make_geo(N);
   em_adjoint_kernel<<<nblocks(g.V2, kAdjThreads), kAdjThreads, 0, st>>>(phi, lam_in, lam_out, g, a, partial, done,
                                                                          g4);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ideal_adjoint(Fields u, Fields lam_in, Fields lam_out, Fields P1, Fields PB, Fields QB, int N,
+                                 const IdealAdjArgs &a, double *partial, unsigned *done, double *g4,
+                                 cudaStream_t st) {
+  const Geo g = make_geo(N);
+  const long long V = 2 * g.V2;
+  rot_phi_kernel<<<nblocks(V, kThreads), kThreads, 0, st>>>(u, P1, V, a.k);
+  ideal_adj_a_kernel<<<nblocks(g.V2, 128), 128, 0, st>>>(u, lam_in, P1, PB, QB, g, a, partial, done, g4);
+  ideal_adj_b_kernel<<<nblocks(g.V2, 128), 128, 0, st>>>(u, lam_out, P1, PB, QB, g, a);
   return cudaGetLastError();
 }
 

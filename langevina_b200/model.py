@@ -162,26 +162,26 @@ class ModelA:
         L.check(self.lib.lgv_get_counter(self.handle, C.byref(c)), "lgv_get_counter")
         return c.value
 
-    def em_forward(self, dt, nsteps, avg_begin, ckpt_every, t=0.0):
-        """Differentiable Euler-Maruyama run (lgv_em_forward): returns the time averages
+    def diff_forward(self, dt, nsteps, avg_begin, ckpt_every, t=0.0, evolver=L.MODELA_EM):
+        """Differentiable run (lgv_diff_forward): returns the time averages
         (sigma, V sum_a pibar_a^2) over steps avg_begin+1 .. nsteps."""
         obs = np.zeros(2)
-        L.check(self.lib.lgv_em_forward(self.handle, float(dt), float(t), int(nsteps), int(avg_begin),
-                                        int(ckpt_every), L.ptr(obs)), "lgv_em_forward")
+        L.check(self.lib.lgv_diff_forward(self.handle, int(evolver), float(dt), float(t), int(nsteps), int(avg_begin),
+                                          int(ckpt_every), L.ptr(obs)), "lgv_diff_forward")
         return obs
 
-    def em_backward(self, w=(1.0, 1.0)):
-        """Gradient of w[0] obs[0] + w[1] obs[1] of the last em_forward with respect to
-        (mass0, lambda, H, gamma), by the adjoint kernels (lgv_em_backward)."""
+    def diff_backward(self, w=(1.0, 1.0)):
+        """Gradient of w[0] obs[0] + w[1] obs[1] of the last diff_forward with respect to
+        (mass0, lambda, H, gamma), by the adjoint kernels (lgv_diff_backward)."""
         w = np.ascontiguousarray(w, dtype=np.float64)
         g = np.zeros(4)
-        L.check(self.lib.lgv_em_backward(self.handle, L.ptr(w), L.ptr(g)), "lgv_em_backward")
+        L.check(self.lib.lgv_diff_backward(self.handle, L.ptr(w), L.ptr(g)), "lgv_diff_backward")
         return g
 
-    def em_averages(self, nsteps):
-        """Volume averages <phi_a>(n), n = 0..nsteps, of the last em_forward, shape (nsteps+1, 4)."""
+    def diff_averages(self, nsteps):
+        """Volume averages <phi_a>(n), n = 0..nsteps, of the last diff_forward, shape (nsteps+1, 4)."""
         out = np.zeros((int(nsteps) + 1, 4))
-        L.check(self.lib.lgv_em_averages(self.handle, L.ptr(out), int(nsteps)), "lgv_em_averages")
+        L.check(self.lib.lgv_diff_averages(self.handle, L.ptr(out), int(nsteps)), "lgv_diff_averages")
         return out
 
     def energy(self):
@@ -241,6 +241,11 @@ class ModelAEulerMaruyama(Stepper):
     evolver = L.MODELA_EM
 
 
+class IdealEulerMaruyama(Stepper):
+    """Ideal step then Euler-Maruyama relaxation of phi (no counterpart in the reference)."""
+    evolver = L.IDEAL_EM
+
+
 class PV2HBSplit(Stepper):
     """PV2HBSplit (Stepper.h:176-211): scounts = (inner, outer)."""
 
@@ -266,6 +271,8 @@ def make_stepper(model, evolverType):
         return PV2HBSplit(model, (1, 1))
     if evolverType == "ModelAEulerMaruyama":
         return ModelAEulerMaruyama(model)
+    if evolverType == "IdealEulerMaruyama":
+        return IdealEulerMaruyama(model)
     if evolverType == "EulerLangevinHB":
         return EulerLangevinHB(model)
     raise ValueError(f"Unrecognized stepper type {evolverType}")

@@ -803,6 +803,10 @@ static void step_once(Handle &h, int ev, int inner, int outer, double dt, double
     case LGV_EULER_LANGEVIN_HB: hb_sweep(h, dt, mass); break;
     case LGV_CHARGE_HB: charge_hb(h, dt); break;
     case LGV_MODELA_EM: em_step(h, dt, mass); break;
+    case LGV_IDEAL_EM:  // no counterpart in the reference: the ideal step, then Euler-Maruyama
+      ideal_step(h, dt);
+      em_step(h, dt, mass);
+      break;
     default: throw std::string("step: unknown evolver");
   }
 }

@@ -1,8 +1,10 @@
-"""GPU checks of the differentiable Euler-Maruyama Model A path
-(lgv_em_forward / lgv_em_backward and the torch.autograd.Function over them).
+"""GPU checks of the differentiable runs (lgv_diff_forward / lgv_diff_backward
+and the torch.autograd.Function over them): Euler-Maruyama Model A ("em"),
+the ideal O(4) rotation step ("ideal") and the two in sequence ("ideal_em").
 
 - the time averages and the adjoint gradient against the numpy restatement of
-  the run and its adjoint (oracle/em_adjoint.py), on the same counter noise;
+  the runs and their adjoints (oracle/diff_adjoint.py), on the same counter
+  noise;
 - the gradient with respect to (m^2, lambda, H, Gamma) against central finite
   differences, h = 1e-5, with common random numbers (same state, same seed and
   counter), within 1e-6 relative: on small lattices and on the 48^3, 2000-step
@@ -21,6 +23,7 @@ pytestmark = pytest.mark.gpu
 
 SEED = 977
 CFG4 = dict(mass0=-4.813, lam=10.0, H=0.01, gamma=1.0)  # (m^2, lambda, H, Gamma) of the 48^3 run
+EVOLVER = {"em": 6, "ideal": 3, "ideal_em": 7}
 
 
 def theta_of(c):
@@ -32,21 +35,23 @@ def kw_of(theta):
 
 
 class EmLattice(GpuLattice):
+    scheme = "em"
+
     def forward(self, dt, S, b, K, t=0.0):
         obs = np.zeros(2)
-        self.L.check(self.lib.lgv_em_forward(self.h, float(dt), float(t), int(S), int(b), int(K), self.L.ptr(obs)),
-                     "em_forward")
+        self.L.check(self.lib.lgv_diff_forward(self.h, EVOLVER[self.scheme], float(dt), float(t), int(S), int(b),
+                                               int(K), self.L.ptr(obs)), "diff_forward")
         return obs
 
     def backward(self, w=(1.0, 1.0)):
         w = np.ascontiguousarray(w, dtype=np.float64)
         g = np.zeros(4)
-        self.L.check(self.lib.lgv_em_backward(self.h, self.L.ptr(w), self.L.ptr(g)), "em_backward")
+        self.L.check(self.lib.lgv_diff_backward(self.h, self.L.ptr(w), self.L.ptr(g)), "diff_backward")
         return g
 
     def averages(self, S):
         out = np.zeros((S + 1, 4))
-        self.L.check(self.lib.lgv_em_averages(self.h, self.L.ptr(out), int(S)), "em_averages")
+        self.L.check(self.lib.lgv_diff_averages(self.h, self.L.ptr(out), int(S)), "diff_averages")
         return out
 
     def set_theta(self, theta, **extra):
@@ -77,42 +82,70 @@ def assert_grad_close(g, ref, rtol, what):
     return err
 
 
-@pytest.mark.parametrize("N,S,b,K", [(8, 40, 15, 7), (6, 25, 0, 25), (10, 33, 32, 4)])
-def test_adjoint_matches_numpy_restatement(lgv, oracle_mod, N, S, b, K):
-    import em_adjoint as ema
+@pytest.mark.parametrize("scheme,N,S,b,K", [("em", 8, 40, 15, 7), ("em", 6, 25, 0, 25), ("em", 10, 33, 32, 4),
+                                             ("ideal", 8, 30, 10, 7), ("ideal", 6, 12, 0, 12),
+                                             ("ideal_em", 8, 40, 15, 7), ("ideal_em", 10, 21, 3, 5)])
+def test_adjoint_matches_numpy_restatement(lgv, oracle_mod, scheme, N, S, b, K):
+    import diff_adjoint as da
 
     theta = theta_of(CFG4)
+    theta[2] = 0.3  # a larger H so the ideal step's -H phi source is visible
     lat = EmLattice(lgv, N, seed=SEED, dmassdt=-0.3, **kw_of(theta))
+    lat.scheme = scheme
     u = rand_state(N, 3 + N)
     lat.set_state(u)
     lat.counter(5)
     dt, t0 = 0.02, 0.5
     obs = lat.forward(dt, S, b, K, t=t0)
-    assert lat.counter() == 5 + S
-    phis = ema.em_run(u[..., :4], theta, dt, S, SEED, 5, t0=t0, dmassdt=-0.3)
-    np.testing.assert_allclose(lat.get_state()[..., :4], phis[-1], rtol=1e-12, atol=1e-12)
-    np.testing.assert_array_equal(lat.get_state()[..., 4:], u[..., 4:])
-    np.testing.assert_allclose(obs, ema.observables(phis, b), rtol=1e-12, atol=1e-14)
+    assert lat.counter() == 5 + (S if scheme != "ideal" else 0)
+    run = da.Run(scheme, theta, dt, SEED, 5, t0=t0, dmassdt=-0.3)
+    us = run.forward(u, S)
+    np.testing.assert_allclose(lat.get_state(), us[-1], rtol=1e-11, atol=1e-11)
+    if scheme == "em":
+        np.testing.assert_array_equal(lat.get_state()[..., 4:], u[..., 4:])
+    np.testing.assert_allclose(obs, da.Run.observables(us, b), rtol=1e-11, atol=1e-13)
     avg = lat.averages(S)
-    np.testing.assert_allclose(avg, np.array([p.mean(axis=(0, 1, 2)) for p in phis]), rtol=1e-12, atol=1e-14)
+    np.testing.assert_allclose(avg, np.array([x[..., :4].mean(axis=(0, 1, 2)) for x in us]), rtol=1e-11, atol=1e-13)
     for w in [(1.0, 1.0), (0.5, -2.0), (0.0, 1.0)]:
         g = lat.backward(w)
-        ref = ema.em_gradient(phis, theta, dt, b, SEED, 5, w=w, t0=t0, dmassdt=-0.3)
-        assert_grad_close(g, ref, 1e-10, f"adjoint vs numpy restatement N={N} w={w}")
+        ref = run.gradient(us, b, w=w)
+        assert_grad_close(g, ref, 1e-9, f"{scheme} adjoint vs numpy restatement N={N} w={w}")
+        if scheme == "ideal":
+            assert g[0] == 0 and g[1] == 0 and g[3] == 0
 
 
-@pytest.mark.parametrize("N,S,b,K", [(16, 400, 200, 50), (12, 300, 100, 64)])
-def test_adjoint_matches_central_fd_small(lgv, N, S, b, K):
+@pytest.mark.parametrize("scheme,N,S,b,K", [("em", 16, 400, 200, 50), ("em", 12, 300, 100, 64),
+                                             ("ideal_em", 16, 300, 100, 50), ("ideal", 12, 200, 50, 40)])
+def test_adjoint_matches_central_fd_small(lgv, scheme, N, S, b, K):
     theta = theta_of(CFG4)
+    if scheme == "ideal":
+        theta[2] = 0.3
     lat = EmLattice(lgv, N, seed=SEED, **kw_of(theta))
-    u = rand_state(N, 21, charges=False)
+    lat.scheme = scheme
+    u = rand_state(N, 21, charges=(scheme != "em"))
     run = (0.02, S, b, K)
     lat.set_state(u)
     lat.counter(0)
     lat.forward(*run)
     g = lat.backward((1.0, 1.0))
     fd = central_fd(lat, u, 0, theta, run)
-    assert_grad_close(g, fd, 1e-6, f"adjoint vs central FD N={N}")
+    assert_grad_close(g, fd, 1e-6, f"{scheme} adjoint vs central FD N={N}")
+
+
+def test_ideal_em_step_matches_oracle(lgv, oracle_mod):
+    """lgv_step with LGV_IDEAL_EM against the oracle's ideal step then Euler-Maruyama step."""
+    N = 8
+    c = dict(CFG4, chi=5.0, seed=SEED)
+    g = GpuLattice(lgv, N, **c)
+    o = oracle_mod.Oracle(N, mode=oracle_mod.COUNTER, **c)
+    u = rand_state(N, 77)
+    g.set_state(u)
+    o.set_state(u)
+    g.step(7, 0.02, t=0.1, nsteps=4)
+    o.step(7, 0.02, t=0.1, nsteps=4)
+    from lgvtest import assert_state_close
+    assert_state_close(g.get_state(), o.get_state(), what="ideal + EM")
+    assert g.counter() == 4
 
 
 def test_adjoint_matches_central_fd_48cubed_2000_steps(lgv):
@@ -152,12 +185,14 @@ def test_adjoint_errors(lgv):
     N = 4
     lat = EmLattice(lgv, N, seed=SEED, **CFG4)
     w, g = np.ones(2), np.zeros(4)
-    assert lat.lib.lgv_em_backward(lat.h, lat.L.ptr(w), lat.L.ptr(g)) != 0  # no forward yet
+    assert lat.lib.lgv_diff_backward(lat.h, lat.L.ptr(w), lat.L.ptr(g)) != 0  # no forward yet
     obs = np.zeros(2)
-    assert lat.lib.lgv_em_forward(lat.h, 0.02, 0.0, 10, 10, 5, lat.L.ptr(obs)) != 0  # avg_begin == nsteps
-    assert lat.lib.lgv_em_forward(lat.h, 0.02, 0.0, 10, 0, 0, lat.L.ptr(obs)) != 0  # ckpt_every 0
+    assert lat.lib.lgv_diff_forward(lat.h, 6, 0.02, 0.0, 10, 10, 5, lat.L.ptr(obs)) != 0  # avg_begin == nsteps
+    assert lat.lib.lgv_diff_forward(lat.h, 6, 0.02, 0.0, 10, 0, 0, lat.L.ptr(obs)) != 0  # ckpt_every 0
+    assert lat.lib.lgv_diff_forward(lat.h, 4, 0.02, 0.0, 10, 0, 5, lat.L.ptr(obs)) != 0  # Metropolis: no adjoint
     lat.mode(1)
-    assert lat.lib.lgv_em_forward(lat.h, 0.02, 0.0, 10, 0, 5, lat.L.ptr(obs)) != 0  # injected noise
+    assert lat.lib.lgv_diff_forward(lat.h, 6, 0.02, 0.0, 10, 0, 5, lat.L.ptr(obs)) != 0  # injected noise
+    assert lat.lib.lgv_diff_forward(lat.h, 3, 0.02, 0.0, 10, 0, 5, lat.L.ptr(obs)) == 0  # ideal: no noise needed
 
 
 def _model(lgv, N, theta, seed=SEED):
@@ -169,7 +204,7 @@ def _model(lgv, N, theta, seed=SEED):
 def test_autograd_function_gradcheck(lgv):
     import torch
 
-    from langevina_b200.adjoint import em_observables
+    from langevina_b200.adjoint import diff_observables, em_observables
 
     N = 8
     model = _model(lgv, N, theta_of(CFG4))
@@ -186,14 +221,14 @@ def test_autograd_function_gradcheck(lgv):
 
     obs = f(theta)
     (obs[0] + obs[1]).backward()
-    lat_g = model.em_backward((1.0, 1.0))
+    lat_g = model.diff_backward((1.0, 1.0))
     assert np.array_equal(theta.grad.numpy(), lat_g)
 
 
 def test_autograd_backward_after_another_forward(lgv):
     import torch
 
-    from langevina_b200.adjoint import em_observables
+    from langevina_b200.adjoint import diff_observables, em_observables
 
     N = 8
     model = _model(lgv, N, theta_of(CFG4))
@@ -202,7 +237,7 @@ def test_autograd_backward_after_another_forward(lgv):
     model.set_counter(0)
     th1 = torch.tensor(theta_of(CFG4), dtype=torch.float64, requires_grad=True)
     o1 = em_observables(model, th1, 0.02, 40, 10, ckpt_every=8)
-    expect = model.em_backward((1.0, 1.0))
+    expect = model.diff_backward((1.0, 1.0))
     th2 = torch.tensor(theta_of(CFG4) * 1.01, dtype=torch.float64, requires_grad=True)
     o2 = em_observables(model, th2, 0.02, 30, 5, ckpt_every=8)
     state2, ctr2 = model.get_state(), model.get_counter()
@@ -211,6 +246,25 @@ def test_autograd_backward_after_another_forward(lgv):
     assert np.array_equal(model.get_state(), state2) and model.get_counter() == ctr2
     o2.sum().backward()
     assert th2.grad is not None and np.all(np.isfinite(th2.grad.numpy()))
+
+
+def test_autograd_ideal_em_gradcheck(lgv):
+    import torch
+
+    from langevina_b200.adjoint import diff_observables
+
+    N = 8
+    th0 = theta_of(CFG4)
+    model = _model(lgv, N, th0)
+    u = rand_state(N, 12)
+
+    def f(theta):
+        model.set_state(u)
+        model.set_counter(0)
+        return diff_observables(model, theta, 0.02, 40, 10, ckpt_every=9, evolver="ideal_em")
+
+    theta = torch.tensor(th0, dtype=torch.float64, requires_grad=True)
+    assert torch.autograd.gradcheck(f, (theta,), eps=1e-5, atol=1e-9, rtol=1e-6)
 
 
 def test_fluctuation_dissipation_susceptibility(lgv):
