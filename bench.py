@@ -314,6 +314,97 @@ def run_adjoint(reps=3):
     }
 
 
+ADJ_BATCH = dict(R=32, N=32, steps=1000, avg_begin=500, ckpt=50, dt=0.02, mass0=-4.813, lam=10.0, H=0.003, gamma=1.0)
+
+
+def run_adjoint_batch(reps=3):
+    """Batched adjoint: 32 Euler-Maruyama Model A replicas at 32^3 (distinct
+    seeds), 1000 steps, loss averaged over steps 501..1000, checkpoints every
+    50 steps, all replicas in one launch per step.  Times the plain batched
+    forward (lgv_ensemble_step), the differentiable batched forward and the
+    batched adjoint with CUDA events, and the same 32 gradients taken one
+    replica at a time through lgv_diff_forward / lgv_diff_backward."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+    from langevina_b200 import _lib as L
+
+    lib = L.load()
+    c = ADJ_BATCH
+    R, N, S = c["R"], c["N"], c["steps"]
+    kw = dict(mass0=c["mass0"], lam=c["lam"], H=c["H"], gamma=c["gamma"])
+    arr = (L.lgv_params * R)()
+    for r in range(R):
+        arr[r] = L.make_params(N, seed=7000 + r, **kw)
+    e = C.c_void_p()
+    L.check(lib.lgv_ensemble_create(R, arr, C.byref(e)), "ensemble_create")
+    stream = torch.cuda.Stream()
+    L.check(lib.lgv_ensemble_set_stream(e, C.c_void_p(stream.cuda_stream)), "ens stream")
+    L.check(lib.lgv_ensemble_initialize(e, L.INIT_PHI_GAUSSIAN, 0.1), "init")
+    obs = np.zeros((R, 2))
+    w = np.ones((R, 2))
+    g = np.zeros((R, 4))
+
+    def timed(fn, st):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(st)
+        fn()
+        e1.record(st)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    def plain():
+        L.check(lib.lgv_ensemble_step(e, L.MODELA_EM, 1, 1, c["dt"], 0.0, S), "ens step")
+
+    def fwd():
+        L.check(lib.lgv_ensemble_diff_forward(e, c["dt"], 0.0, S, c["avg_begin"], c["ckpt"], L.ptr(obs)), "fwd")
+
+    def bwd():
+        L.check(lib.lgv_ensemble_diff_backward(e, L.ptr(w), L.ptr(g)), "bwd")
+
+    fwd(), bwd(), plain()
+    tp, tf, tb = [], [], []
+    for _ in range(reps):
+        tp.append(timed(plain, stream))
+        tf.append(timed(fwd, stream))
+        tb.append(timed(bwd, stream))
+    lib.lgv_ensemble_destroy(e)
+
+    # one replica at a time through the single-lattice differentiable path
+    h = C.c_void_p()
+    p0 = L.make_params(N, seed=7000, **kw)
+    L.check(lib.lgv_create(C.byref(p0), C.byref(h)), "create")
+    s1 = torch.cuda.Stream()
+    L.check(lib.lgv_set_stream(h, C.c_void_p(s1.cuda_stream)), "stream")
+    o1, g1 = np.zeros(2), np.zeros(4)
+
+    def loop():
+        for r in range(R):
+            pr = L.make_params(N, seed=7000 + r, **kw)
+            L.check(lib.lgv_set_params(h, C.byref(pr)), "params")
+            L.check(lib.lgv_initialize(h, L.INIT_PHI_GAUSSIAN, 0.1), "init")
+            L.check(lib.lgv_diff_forward(h, L.MODELA_EM, c["dt"], 0.0, S, c["avg_begin"], c["ckpt"], L.ptr(o1)), "f")
+            L.check(lib.lgv_diff_backward(h, L.ptr(w[0]), L.ptr(g1)), "b")
+
+    loop()
+    tl = timed(loop, s1)
+    lib.lgv_destroy(h)
+    tp, tf, tb = min(tp), min(tf), min(tb)
+    return {
+        "workload": f"{R} Euler-Maruyama Model A replicas at {N}^3 FP64, distinct seeds, {S} steps, dt={c['dt']}, "
+                    f"loss over steps {c['avg_begin'] + 1}..{S}, checkpoints every {c['ckpt']}, "
+                    f"m^2={c['mass0']}, lambda={c['lam']}, H={c['H']}, Gamma={c['gamma']}",
+        "plain_batched_forward_ms": tp, "diff_batched_forward_ms": tf, "batched_adjoint_ms": tb,
+        "adjoint_over_forward": tb / tp, "forward_plus_adjoint_over_forward": (tf + tb) / tp,
+        "gradients_per_s": R * 1e3 / (tf + tb),
+        "one_replica_at_a_time_ms": tl, "one_replica_at_a_time_gradients_per_s": R * 1e3 / tl,
+        "speedup_vs_one_at_a_time": tl / (tf + tb),
+        "timing": "CUDA events, best of %d (batched); one pass (one replica at a time, incl. init)" % reps,
+    }
+
+
 def run_ours(a):
     import ctypes as C
 
@@ -463,6 +554,7 @@ def run_ours(a):
     adjoint = None
     if world == 1 and not a.no_adjoint:
         adjoint = run_adjoint()
+        adjoint["batched"] = run_adjoint_batch()
     if dist:
         dist.barrier()
         dist.destroy_process_group()

@@ -286,6 +286,14 @@ int lgv_ensemble_tune(lgv_ensemble *e, int tile, int zchunk, int order);
 int lgv_ensemble_autotune(lgv_ensemble *e, int evolver, int inner, int outer, double dt, int steps, int *choice,
                           double *ms_per_step);
 int lgv_ensemble_use_graphs(lgv_ensemble *e, int enable);
+/* Differentiable Euler-Maruyama Model A runs of all replicas at once (no
+ * counterpart in the reference): one launch per step over all replicas.
+ * Replica r gets what lgv_diff_forward / lgv_diff_backward with evolver
+ * LGV_MODELA_EM return for a single lattice with params[r] and the
+ * ensemble's counter: obs holds [R][2], w [R][2] and grad [R][4]. */
+int lgv_ensemble_diff_forward(lgv_ensemble *e, double dt, double t, int nsteps, int avg_begin, int ckpt_every,
+                              double *obs);
+int lgv_ensemble_diff_backward(lgv_ensemble *e, const double *w, double *grad);
 int lgv_ensemble_set_stream(lgv_ensemble *e, void *cuda_stream);
 int lgv_ensemble_synchronize(lgv_ensemble *e);
 

@@ -100,6 +100,8 @@ SIGNATURES = [
     ("lgv_ensemble_autotune", C.c_int, [_H, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, C.c_void_p,
                                         C.POINTER(C.c_double)]),
     ("lgv_ensemble_use_graphs", C.c_int, [_H, C.c_int]),
+    ("lgv_ensemble_diff_forward", C.c_int, [_H, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, C.c_void_p]),
+    ("lgv_ensemble_diff_backward", C.c_int, [_H, C.c_void_p, C.c_void_p]),
     ("lgv_ensemble_set_stream", C.c_int, [_H, C.c_void_p]),
     ("lgv_ensemble_synchronize", C.c_int, [_H]),
 ]

@@ -73,6 +73,22 @@ struct lgv_ensemble {
   int tile = LGV_TILE_32x8, zchunk = 16, order = LGV_PACK_GIVEN;
   bool graphs = true;
   std::map<std::tuple<int, int, int, double, int, int>, cudaGraphExec_t> cache;
+  // differentiable Euler-Maruyama run (lgv_ensemble_diff_forward / _backward)
+  struct {
+    bool ready = false;
+    double dt = 0;
+    int S = 0, b = 0, K = 1;
+    unsigned long long ctr0 = 0;
+    std::vector<double> tn;
+    std::vector<lgv::DiffDesc> hd;
+    std::vector<double *> bufs;
+    std::vector<size_t> lens;
+    lgv::DiffDesc *dd = nullptr;
+    double *wg = nullptr;  // [R][2] weights then [R][4] gradients
+    double *partial = nullptr;
+    unsigned *done = nullptr;  // one counter per replica
+    size_t partial_len = 0;
+  } diff;
 };
 
 namespace {
@@ -312,6 +328,12 @@ int lgv_ensemble_destroy(lgv_ensemble *e) {
   if (e->dyn) cudaFree(e->dyn);
   if (e->partial) cudaFree(e->partial);
   if (e->oavg) cudaFree(e->oavg);
+  for (double *b : e->diff.bufs)
+    if (b) cudaFree(b);
+  if (e->diff.dd) cudaFree(e->diff.dd);
+  if (e->diff.wg) cudaFree(e->diff.wg);
+  if (e->diff.partial) cudaFree(e->diff.partial);
+  if (e->diff.done) cudaFree(e->diff.done);
   if (e->own) cudaStreamDestroy(e->own);
   delete e;
   return LGV_OK;
@@ -443,6 +465,120 @@ int lgv_ensemble_step(lgv_ensemble *e, int evolver, int inner, int outer, double
     }
   }
   for (; done < nsteps; ++done) ETRY(enqueue_step(e, evolver, inner, outer, dt));
+  return LGV_OK;
+}
+
+int lgv_ensemble_diff_forward(lgv_ensemble *e, double dt, double t, int nsteps, int avg_begin, int ckpt_every,
+                              double *obs) {
+  if (!e || !obs) return efail(LGV_ERR_INVALID, "NULL argument");
+  if (nsteps < 1 || avg_begin < 0 || avg_begin >= nsteps || ckpt_every < 1)
+    return efail(LGV_ERR_INVALID, "lgv_ensemble_diff_forward: need nsteps >= 1, 0 <= avg_begin < nsteps, ckpt_every >= 1");
+  auto &D = e->diff;
+  D.ready = false;
+  const int R = e->R, S = nsteps, K = ckpt_every;
+  const size_t nck = (size_t)(S - 1) / K + 1;
+  if (D.bufs.empty()) {
+    D.bufs.assign(R, nullptr);
+    D.lens.assign(R, 0);
+    D.hd.assign(R, lgv::DiffDesc{});
+    ECK(cudaMalloc((void **)&D.dd, R * sizeof(lgv::DiffDesc)));
+    ECK(cudaMalloc((void **)&D.wg, (size_t)R * 6 * sizeof(double)));
+    ECK(cudaMalloc((void **)&D.done, R * sizeof(unsigned)));
+    ECK(cudaMemsetAsync(D.done, 0, R * sizeof(unsigned), e->stream));
+  }
+  const size_t need_partial = (size_t)e->plane_map.nblocks * 4 + 16;
+  if (D.partial_len < need_partial) {
+    if (D.partial) cudaFree(D.partial);
+    D.partial = nullptr;
+    D.partial_len = 0;
+    ECK(cudaMalloc((void **)&D.partial, need_partial * sizeof(double)));
+    D.partial_len = need_partial;
+  }
+  for (int r = 0; r < R; ++r) {
+    const size_t V = (size_t)e->p[r].N * e->p[r].N * e->p[r].N;
+    // checkpoints, segment states, two adjoint states, averages
+    const size_t need = (nck + (size_t)K + 2) * 4 * V + (size_t)(S + 1) * 4;
+    if (D.lens[r] < need) {
+      if (D.bufs[r]) cudaFree(D.bufs[r]);
+      D.bufs[r] = nullptr;
+      D.lens[r] = 0;
+      ECK(cudaMalloc((void **)&D.bufs[r], need * sizeof(double)));
+      D.lens[r] = need;
+    }
+    lgv::DiffDesc &d = D.hd[r];
+    d.V = (long long)V;
+    d.ckpt = D.bufs[r];
+    d.seg = d.ckpt + nck * 4 * V;
+    d.lam = d.seg + (size_t)K * 4 * V;
+    d.avg = d.lam + 8 * V;
+    d.w = D.wg + 2 * r;
+    d.grad = D.wg + 2 * R + 4 * r;
+  }
+  ECK(cudaMemcpyAsync(D.dd, D.hd.data(), R * sizeof(lgv::DiffDesc), cudaMemcpyHostToDevice, e->stream));
+  D.dt = dt;
+  D.S = S;
+  D.b = avg_begin;
+  D.K = K;
+  D.ctr0 = e->ctr;
+  D.tn.assign(S + 1, 0.0);
+  D.tn[0] = t;
+  for (int n = 0; n < S; ++n) D.tn[n + 1] = D.tn[n] + dt;
+  const BlockMap &pm = e->plane_map;
+  for (int r = 0; r < R; ++r)
+    ECK(lgv::launch_phi_avg(cur_fields(e, r), e->p[r].N, D.partial, D.done, D.hd[r].avg, e->stream));
+  for (int n = 0; n < S; ++n) {
+    if (n % K == 0)
+      ECK(lgv::launch_batch_diff_copy(e->dd, D.dd, pm.rep, pm.first, pm.nblocks, 0, e->phase_phi, n / K, avg_begin, S,
+                                      e->stream));
+    ECK(lgv::launch_batch_em_fwd(e->dd, D.dd, pm.rep, pm.first, pm.count, pm.nblocks, e->phase_phi, D.ctr0 + n,
+                                 D.tn[n], dt, n, D.partial, D.done, e->stream));
+    e->phase_phi ^= 1;
+  }
+  e->ctr += (unsigned long long)S;
+  std::vector<double> avg((size_t)(S + 1) * 4);
+  for (int r = 0; r < R; ++r) {
+    ECK(cudaMemcpyAsync(avg.data(), D.hd[r].avg, avg.size() * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+    ECK(cudaStreamSynchronize(e->stream));
+    const double Vd = (double)D.hd[r].V;
+    double o0 = 0, o1 = 0;
+    for (int n = avg_begin + 1; n <= S; ++n) {
+      const double *a = &avg[(size_t)n * 4];
+      o0 += a[0];
+      o1 += Vd * (a[1] * a[1] + a[2] * a[2] + a[3] * a[3]);
+    }
+    obs[2 * r] = o0 / (double)(S - avg_begin);
+    obs[2 * r + 1] = o1 / (double)(S - avg_begin);
+  }
+  D.ready = true;
+  return LGV_OK;
+}
+
+int lgv_ensemble_diff_backward(lgv_ensemble *e, const double *w, double *grad) {
+  if (!e || !w || !grad) return efail(LGV_ERR_INVALID, "NULL argument");
+  auto &D = e->diff;
+  if (!D.ready) return efail(LGV_ERR_STATE, "lgv_ensemble_diff_backward: no forward run to differentiate");
+  const int R = e->R, S = D.S, K = D.K;
+  const BlockMap &pm = e->plane_map;
+  ECK(cudaMemcpyAsync(D.wg, w, (size_t)R * 2 * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+  ECK(cudaMemsetAsync(D.wg + 2 * R, 0, (size_t)R * 4 * sizeof(double), e->stream));
+  ECK(lgv::launch_batch_diff_copy(e->dd, D.dd, pm.rep, pm.first, pm.nblocks, 2, 0, 0, D.b, S, e->stream));
+  int cur = 0, loaded = -1;
+  for (int n = S - 1; n >= 0; --n) {
+    const int s = n / K;
+    if (s != loaded) {
+      ECK(lgv::launch_batch_diff_copy(e->dd, D.dd, pm.rep, pm.first, pm.nblocks, 1, 0, s, D.b, S, e->stream));
+      const int last = std::min(s * K + K - 1, S - 1);
+      for (int m = s * K; m < last; ++m)
+        ECK(lgv::launch_batch_em_seg(e->dd, D.dd, pm.rep, pm.first, pm.nblocks, m - s * K, D.ctr0 + m, D.tn[m], D.dt,
+                                     e->stream));
+      loaded = s;
+    }
+    ECK(lgv::launch_batch_em_adj(e->dd, D.dd, pm.rep, pm.first, pm.count, pm.nblocks, n - s * K, cur, n, D.b, S,
+                                 D.ctr0 + n, D.tn[n], D.dt, D.partial, D.done, e->stream));
+    cur ^= 1;
+  }
+  ECK(cudaMemcpyAsync(grad, D.wg + 2 * R, (size_t)R * 4 * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+  ECK(cudaStreamSynchronize(e->stream));
   return LGV_OK;
 }
 

@@ -88,6 +88,32 @@ struct EnsDyn {
 };
 
 
+// Differentiable Euler-Maruyama runs of an ensemble: per-replica buffers of
+// V-double planes.  ckpt: checkpoint slots of 4 planes; seg: the K states of
+// the segment being differentiated; lam: two 4-plane adjoint states; avg:
+// (S+1) x 4 volume averages; w: the replica's observable weights.
+struct DiffDesc {
+  double *ckpt, *seg, *lam, *avg, *w, *grad;
+  long long V;
+};
+
+// forward step n: phi of the lattice buffer `phase` -> phase ^ 1, averages into avg[n+1]
+cudaError_t launch_batch_em_fwd(const RepDesc *d, const DiffDesc *dd, const int *rep, const int *first,
+                                const int *count, int nblocks, int phase, unsigned long long ctr, double t, double dt,
+                                int n, double *partial, unsigned *done, cudaStream_t st);
+// recompute: seg slot m -> m + 1
+cudaError_t launch_batch_em_seg(const RepDesc *d, const DiffDesc *dd, const int *rep, const int *first, int nblocks,
+                                int m, unsigned long long ctr, double t, double dt, cudaStream_t st);
+// adjoint of step n at seg slot m: lam[cur] -> lam[cur ^ 1], gradients into grad
+cudaError_t launch_batch_em_adj(const RepDesc *d, const DiffDesc *dd, const int *rep, const int *first,
+                                const int *count, int nblocks, int m, int cur, int n, int b, int S,
+                                unsigned long long ctr, double t, double dt, double *partial, unsigned *done,
+                                cudaStream_t st);
+// phi planes: lattice buffer `phase` -> ckpt slot s (dir 0); ckpt slot s -> seg slot 0 (dir 1);
+// lam[0] = dJ/dphi(S) from avg and w (dir 2)
+cudaError_t launch_batch_diff_copy(const RepDesc *d, const DiffDesc *dd, const int *rep, const int *first,
+                                   int nblocks, int dir, int phase, int s, int b, int S, cudaStream_t st);
+
 // phase_phi / phase_q: which buffer holds the current phi / charges
 cudaError_t launch_batch_ideal(const RepDesc *d, const int *rep, const int *first, int nblocks, int tile,
                                int phase_phi, int phase_q, double dt, cudaStream_t st);

@@ -825,6 +825,62 @@ __global__ void __launch_bounds__(kThreads) em_kernel(Fields in, Fields out, Geo
   if (AVG) grid_sum4<kThreads>(acc, partial, done, avg_out, 1.0 / (2.0 * (double)g.V2), false);
 }
 
+// Adjoint of the Euler-Maruyama step for one site pair (see em_adjoint_kernel).
+// Both parities of site pair (m, j, k); adds the parameter sums into v[0..3].
+__device__ __forceinline__ void em_adjoint_pair(const Fields &phi, const Fields &lin, const Fields &lout, const Geo &g,
+                                                const EmAdjArgs &a, int m, int j, int k, double (&v)[4]) {
+  const int H = g.H, N = g.N;
+  const long long row = ((long long)k * N + j) * H;
+  const long long rjp = ((long long)k * N + wrap_inc(j, N)) * H;
+  const long long rjm = ((long long)k * N + wrap_dec(j, N)) * H;
+  const long long rkp = ((long long)wrap_inc(k, N) * N + j) * H;
+  const long long rkm = ((long long)wrap_dec(k, N) * N + j) * H;
+  double gm = 0, gla = 0, gh = 0, gg = 0;
+#pragma unroll
+  for (int parity = 0; parity < 2; ++parity) {
+    const int s = (parity + j + k) & 1;
+    int xm = m - 1 + s, xp = m + s;
+    if (xm < 0) xm += H;
+    if (xp == H) xp = 0;
+    const long long own = (long long)parity * g.V2 + row + m;
+    const long long ob = (long long)(parity ^ 1) * g.V2;
+    const long long nat = ((long long)k * N + j) * N + 2 * m + s;
+    double c[4], l[4];
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      c[b] = phi.c[b][own];
+      l[b] = lin.c[b][own];
+    }
+    Xoro rng = stream_at(a.sk, (uint64_t)nat);
+    double xi[4];
+    const uint64_t r1 = rng.next(), r2 = rng.next(), r3 = rng.next(), r4 = rng.next();
+    box_muller(r1, r2, xi[0], xi[1]);
+    box_muller(r3, r4, xi[2], xi[3]);
+    const double p2 = c[0] * c[0] + c[1] * c[1] + c[2] * c[2] + c[3] * c[3];
+    const double dot = c[0] * l[0] + c[1] * l[1] + c[2] * l[2] + c[3] * l[3];
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const double *P = phi.c[b], *Lm = lin.c[b];
+      const double hf = (P[ob + row + xp] + P[ob + row + xm]) + (P[ob + rjp + m] + P[ob + rjm + m]) +
+                        (P[ob + rkp + m] + P[ob + rkm + m]);
+      const double nl = (Lm[ob + row + xp] + Lm[ob + row + xm]) + (Lm[ob + rjp + m] + Lm[ob + rjm + m]) +
+                        (Lm[ob + rkp + m] + Lm[ob + rkm + m]);
+      const double jl = a.c6 * l[b] + a.lambda * (p2 * l[b] + 2.0 * c[b] * dot) - nl;
+      lout.c[b][own] = l[b] - a.dtg * jl + a.gl[b];
+      double F = -hf + a.c6 * c[b] + a.lambda * p2 * c[b];
+      if (b == 0) F -= a.H;
+      gg += l[b] * (-a.dt * F + a.cxi * xi[b]);
+    }
+    gm += -a.dtg * dot;
+    gla += -a.dtg * p2 * dot;
+    gh += a.dtg * l[0];
+  }
+  v[0] += gm;
+  v[1] += gla;
+  v[2] += gh;
+  v[3] += gg;
+}
+
 // ----------------------------------------------------------------------------
 // Fused ideal step (IdealPV2::step_no_reject, Stepper.cxx:68-176).
 // A CTA owns a TX x TY column of sites and marches up a z-chunk.  At plane p
@@ -1361,6 +1417,152 @@ __global__ void __launch_bounds__(128) batch_charge_kernel(const RepDesc *__rest
   charge_link_site<false, false>(rep_fields(R, phase, phase), R.g, dir, eoA, a, m, j, k, mon);
 }
 
+// ---- differentiable Euler-Maruyama runs of an ensemble ---------------------
+// Per-replica sums of v[0..3] over the replica's blocks first[r] ..
+// first[r] + count[r] - 1 (contiguous in the grid): the replica's last block to
+// finish adds the block partials in block order into out[0..3] (accumulating
+// when add).  done[r] is zero on entry and re-armed.
+__device__ __forceinline__ void rep_sum4(double (&v)[4], int r, int local, int nloc, double *partial, unsigned *done,
+                                         double *out, double scale, bool add) {
+  constexpr int NW = 4;  // 128 threads
+  __shared__ double sm[4][NW];
+  __shared__ bool last;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    warp_sum(v[q]);
+    if (lane == 0) sm[q][warp] = v[q];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) partial[(size_t)blockIdx.x * 4 + q] = ((sm[q][0] + sm[q][1]) + sm[q][2]) + sm[q][3];
+    __threadfence();
+    last = atomicAdd(done + r, 1u) == (unsigned)(nloc - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  const size_t b0 = (size_t)(blockIdx.x - local);
+  if (warp < 4) {
+    double t = 0;
+    for (int b = lane; b < nloc; b += 32) t += __ldcg(partial + (b0 + b) * 4 + warp);
+    warp_sum(t);
+    if (lane == 0) out[warp] = add ? out[warp] + t * scale : t * scale;
+  }
+  if (threadIdx.x == 0) done[r] = 0u;
+}
+
+__device__ __forceinline__ Fields diff_planes(double *base, long long V, long long first) {
+  Fields f{};
+#pragma unroll
+  for (int l = 0; l < 4; ++l) f.c[l] = base + (first + l) * V;
+  return f;
+}
+
+__device__ __forceinline__ EmArgs rep_em_args(const RepDesc &R, unsigned long long ctr, double t, double dt) {
+  EmArgs a{};
+  a.c6 = 6.0 + __dadd_rn(R.mass0, __dmul_rn(R.dmassdt, t));
+  a.dtg = dt * R.gamma;
+  a.sq = sqrt(2.0 * R.gamma * dt);
+  a.lambda = R.lambda;
+  a.H = R.H;
+  a.sk = sub_key(R.key, ctr);
+  return a;
+}
+
+__global__ void __launch_bounds__(128) batch_em_fwd_kernel(const RepDesc *__restrict__ d, const DiffDesc *__restrict__ dd,
+                                                           const int *__restrict__ rep, const int *__restrict__ first,
+                                                           const int *__restrict__ count, int phase,
+                                                           unsigned long long ctr, double t, double dt, int n,
+                                                           double *partial, unsigned *done) {
+  const int r = rep[blockIdx.x];
+  const RepDesc &R = d[r];
+  const DiffDesc &D = dd[r];
+  const int local = blockIdx.x - first[r];
+  int m, j, k;
+  double acc[4] = {0, 0, 0, 0};
+  if (plane_coords(R, local, m, j, k))
+    em_pair<false>(rep_fields(R, phase, phase), rep_fields(R, phase ^ 1, phase ^ 1), R.g, rep_em_args(R, ctr, t, dt), m,
+                   j, k, acc);
+  rep_sum4(acc, r, local, count[r], partial, done, D.avg + (size_t)(n + 1) * 4, 1.0 / (double)D.V, false);
+}
+
+__global__ void __launch_bounds__(128) batch_em_seg_kernel(const RepDesc *__restrict__ d, const DiffDesc *__restrict__ dd,
+                                                           const int *__restrict__ rep, const int *__restrict__ first,
+                                                           int slot, unsigned long long ctr, double t, double dt) {
+  const int r = rep[blockIdx.x];
+  const RepDesc &R = d[r];
+  const DiffDesc &D = dd[r];
+  int m, j, k;
+  if (!plane_coords(R, blockIdx.x - first[r], m, j, k)) return;
+  double acc[4] = {0, 0, 0, 0};
+  em_pair<false>(diff_planes(D.seg, D.V, 4LL * slot), diff_planes(D.seg, D.V, 4LL * (slot + 1)), R.g,
+                 rep_em_args(R, ctr, t, dt), m, j, k, acc);
+}
+
+// dJ/dphi_a(n) of J = w0 obs0 + w1 obs1 (the per-replica averages of the run)
+__device__ __forceinline__ void rep_gl(const DiffDesc &D, int n, int b, int S, double gl[4]) {
+  gl[0] = gl[1] = gl[2] = gl[3] = 0.0;
+  if (n <= b) return;
+  const double M = (double)(S - b);
+  gl[0] = D.w[0] / ((double)D.V * M);
+#pragma unroll
+  for (int a = 1; a < 4; ++a) gl[a] = D.w[1] * 2.0 * D.avg[(size_t)n * 4 + a] / M;
+}
+
+__global__ void __launch_bounds__(128, 4) batch_em_adj_kernel(const RepDesc *__restrict__ d,
+                                                              const DiffDesc *__restrict__ dd,
+                                                              const int *__restrict__ rep,
+                                                              const int *__restrict__ first,
+                                                              const int *__restrict__ count, int slot, int cur, int n,
+                                                              int b, int S, unsigned long long ctr, double t, double dt,
+                                                              double *partial, unsigned *done) {
+  const int r = rep[blockIdx.x];
+  const RepDesc &R = d[r];
+  const DiffDesc &D = dd[r];
+  const int local = blockIdx.x - first[r];
+  EmAdjArgs a{};
+  a.c6 = 6.0 + __dadd_rn(R.mass0, __dmul_rn(R.dmassdt, t));
+  a.dtg = dt * R.gamma;
+  a.dt = dt;
+  a.lambda = R.lambda;
+  a.H = R.H;
+  a.cxi = sqrt(2.0 * dt) / (2.0 * sqrt(R.gamma));
+  rep_gl(D, n, b, S, a.gl);
+  a.sk = sub_key(R.key, ctr);
+  double v[4] = {0, 0, 0, 0};
+  int m, j, k;
+  if (plane_coords(R, local, m, j, k))
+    em_adjoint_pair(diff_planes(D.seg, D.V, 4LL * slot), diff_planes(D.lam, D.V, 4LL * cur),
+                    diff_planes(D.lam, D.V, 4LL * (cur ^ 1)), R.g, a, m, j, k, v);
+  rep_sum4(v, r, local, count[r], partial, done, D.grad, 1.0, true);
+}
+
+__global__ void __launch_bounds__(128) batch_diff_copy_kernel(const RepDesc *__restrict__ d,
+                                                              const DiffDesc *__restrict__ dd,
+                                                              const int *__restrict__ rep,
+                                                              const int *__restrict__ first, int dir, int phase, int s,
+                                                              int b, int S) {
+  const int r = rep[blockIdx.x];
+  const RepDesc &R = d[r];
+  const DiffDesc &D = dd[r];
+  int m, j, k;
+  if (!plane_coords(R, blockIdx.x - first[r], m, j, k)) return;
+  const long long row = ((long long)k * R.g.N + j) * R.g.H + m;
+  double gl[4];
+  if (dir == 2) rep_gl(D, S, b, S, gl);
+#pragma unroll
+  for (int l = 0; l < 4; ++l)
+#pragma unroll
+    for (int par = 0; par < 2; ++par) {
+      const long long o = par * R.g.V2 + row;
+      if (dir == 0) D.ckpt[((long long)s * 4 + l) * D.V + o] = R.base[phase][l * R.pstride + o];
+      else if (dir == 1) D.seg[(long long)l * D.V + o] = D.ckpt[((long long)s * 4 + l) * D.V + o];
+      else D.lam[(long long)l * D.V + o] = gl[l];
+    }
+}
+
 __global__ void __launch_bounds__(128) batch_em_kernel(const RepDesc *__restrict__ d, const EnsDyn *__restrict__ dyn,
                                                        const int *__restrict__ rep, const int *__restrict__ first,
                                                        int phase_in, double dt, int ctr_off) {
@@ -1468,62 +1670,19 @@ __global__ void batch_oavg_final_kernel(const RepDesc *__restrict__ d, const int
 //   dL/dH += dtG lam_0,  dL/dG += lam . (-dt F + sqrt(2dt)/(2 sqrt G) xi).
 // One thread per site pair, flat over the V/2 pairs; the parameter sums are
 // accumulated into g4[0..3] (grid_sum4).
+// One thread per site pair, flat over the V/2 pairs; the parameter sums are
+// accumulated into g4[0..3] (grid_sum4).
 constexpr int kAdjThreads = 128;
 __global__ void __launch_bounds__(kAdjThreads, 4) em_adjoint_kernel(Fields phi, Fields lin, Fields lout, Geo g,
-                                                                 EmAdjArgs a, double *partial, unsigned *done,
-                                                                 double *g4) {
+                                                                    EmAdjArgs a, double *partial, unsigned *done,
+                                                                    double *g4) {
   const long long idx = (long long)blockIdx.x * kAdjThreads + threadIdx.x;
-  const int H = g.H, N = g.N;
-  double gm = 0, gla = 0, gh = 0, gg = 0;
+  double v[4] = {0, 0, 0, 0};
   if (idx < g.V2) {
     int m, j, k;
     pair_coords(idx, g, m, j, k);
-    const long long row = ((long long)k * N + j) * H;
-    const long long rjp = ((long long)k * N + wrap_inc(j, N)) * H;
-    const long long rjm = ((long long)k * N + wrap_dec(j, N)) * H;
-    const long long rkp = ((long long)wrap_inc(k, N) * N + j) * H;
-    const long long rkm = ((long long)wrap_dec(k, N) * N + j) * H;
-#pragma unroll
-    for (int parity = 0; parity < 2; ++parity) {
-      const int s = (parity + j + k) & 1;
-      int xm = m - 1 + s, xp = m + s;
-      if (xm < 0) xm += H;
-      if (xp == H) xp = 0;
-      const long long own = (long long)parity * g.V2 + row + m;
-      const long long ob = (long long)(parity ^ 1) * g.V2;
-      const long long nat = ((long long)k * N + j) * N + 2 * m + s;
-      double c[4], l[4];
-#pragma unroll
-      for (int b = 0; b < 4; ++b) {
-        c[b] = phi.c[b][own];
-        l[b] = lin.c[b][own];
-      }
-      Xoro rng = stream_at(a.sk, (uint64_t)nat);
-      double xi[4];
-      const uint64_t r1 = rng.next(), r2 = rng.next(), r3 = rng.next(), r4 = rng.next();
-      box_muller(r1, r2, xi[0], xi[1]);
-      box_muller(r3, r4, xi[2], xi[3]);
-      const double p2 = c[0] * c[0] + c[1] * c[1] + c[2] * c[2] + c[3] * c[3];
-      const double dot = c[0] * l[0] + c[1] * l[1] + c[2] * l[2] + c[3] * l[3];
-#pragma unroll
-      for (int b = 0; b < 4; ++b) {
-        const double *P = phi.c[b], *Lm = lin.c[b];
-        const double hf = (P[ob + row + xp] + P[ob + row + xm]) + (P[ob + rjp + m] + P[ob + rjm + m]) +
-                          (P[ob + rkp + m] + P[ob + rkm + m]);
-        const double nl = (Lm[ob + row + xp] + Lm[ob + row + xm]) + (Lm[ob + rjp + m] + Lm[ob + rjm + m]) +
-                          (Lm[ob + rkp + m] + Lm[ob + rkm + m]);
-        const double jl = a.c6 * l[b] + a.lambda * (p2 * l[b] + 2.0 * c[b] * dot) - nl;
-        lout.c[b][own] = l[b] - a.dtg * jl + a.gl[b];
-        double F = -hf + a.c6 * c[b] + a.lambda * p2 * c[b];
-        if (b == 0) F -= a.H;
-        gg += l[b] * (-a.dt * F + a.cxi * xi[b]);
-      }
-      gm += -a.dtg * dot;
-      gla += -a.dtg * p2 * dot;
-      gh += a.dtg * l[0];
-    }
+    em_adjoint_pair(phi, lin, lout, g, a, m, j, k, v);
   }
-  double v[4] = {gm, gla, gh, gg};
   grid_sum4<kAdjThreads>(v, partial, done, g4, 1.0, true);
 }
 
@@ -2013,6 +2172,33 @@ cudaError_t launch_batch_charge(const RepDesc *d, const EnsDyn *dyn, const int *
 cudaError_t launch_batch_em(const RepDesc *d, const EnsDyn *dyn, const int *rep, const int *first, int nblocks,
                             int phase_in, double dt, int ctr_off, cudaStream_t st) {
   batch_em_kernel<<<nblocks, 128, 0, st>>>(d, dyn, rep, first, phase_in, dt, ctr_off);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_em_fwd(const RepDesc *d, const DiffDesc *dd, const int *rep, const int *first,
+                                const int *count, int nblocks, int phase, unsigned long long ctr, double t, double dt,
+                                int n, double *partial, unsigned *done, cudaStream_t st) {
+  batch_em_fwd_kernel<<<nblocks, 128, 0, st>>>(d, dd, rep, first, count, phase, ctr, t, dt, n, partial, done);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_em_seg(const RepDesc *d, const DiffDesc *dd, const int *rep, const int *first, int nblocks,
+                                int m, unsigned long long ctr, double t, double dt, cudaStream_t st) {
+  batch_em_seg_kernel<<<nblocks, 128, 0, st>>>(d, dd, rep, first, m, ctr, t, dt);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_em_adj(const RepDesc *d, const DiffDesc *dd, const int *rep, const int *first,
+                                const int *count, int nblocks, int m, int cur, int n, int b, int S,
+                                unsigned long long ctr, double t, double dt, double *partial, unsigned *done,
+                                cudaStream_t st) {
+  batch_em_adj_kernel<<<nblocks, 128, 0, st>>>(d, dd, rep, first, count, m, cur, n, b, S, ctr, t, dt, partial, done);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_diff_copy(const RepDesc *d, const DiffDesc *dd, const int *rep, const int *first,
+                                   int nblocks, int dir, int phase, int s, int b, int S, cudaStream_t st) {
+  batch_diff_copy_kernel<<<nblocks, 128, 0, st>>>(d, dd, rep, first, dir, phase, s, b, S);
   return cudaGetLastError();
 }
 

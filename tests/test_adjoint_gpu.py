@@ -291,3 +291,50 @@ def test_fluctuation_dissipation_susceptibility(lgv):
     ma, mf = adj.mean(), fdt.mean()
     se = np.sqrt(adj.var(ddof=1) / len(adj) + fdt.var(ddof=1) / len(fdt))
     assert abs(ma - mf) <= 4 * se + 0.01 * mf, f"d<sigma>/dH {ma:.4f} vs V var(sigma) {mf:.4f} (se {se:.4f})"
+
+
+def test_ensemble_adjoint_matches_single_lattices(lgv):
+    """lgv_ensemble_diff_forward/backward over uneven replicas (sizes, seeds,
+    H) against lgv_diff_forward/backward of each replica alone."""
+    from langevina_b200 import _lib as L
+
+    lib = L.load()
+    sizes = [8, 12, 8, 16, 6]
+    specs = [dict(N=N, seed=500 + r, H=(0.003, 0.006, 0.012)[r % 3], mass0=-4.813 + 0.1 * r, lam=10.0, gamma=1.0)
+             for r, N in enumerate(sizes)]
+    R = len(specs)
+    arr = (L.lgv_params * R)()
+    for r, sp in enumerate(specs):
+        arr[r] = L.make_params(sp["N"], seed=sp["seed"], mass0=sp["mass0"], lam=sp["lam"], H=sp["H"],
+                               gamma=sp["gamma"], dmassdt=-0.2)
+    e = C.c_void_p()
+    L.check(lib.lgv_ensemble_create(R, arr, C.byref(e)), "ensemble_create")
+    try:
+        states = [rand_state(sp["N"], 60 + r) for r, sp in enumerate(specs)]
+        for r in range(R):
+            L.check(lib.lgv_ensemble_set_state(e, r, L.ptr(states[r])), "set_state")
+        L.check(lib.lgv_ensemble_set_counter(e, 9), "set_counter")
+        S, b, K, dt, t0 = 50, 20, 16, 0.02, 0.25
+        obs = np.zeros((R, 2))
+        L.check(lib.lgv_ensemble_diff_forward(e, dt, t0, S, b, K, L.ptr(obs)), "ensemble_diff_forward")
+        w = np.array([[1.0, 1.0], [0.5, -1.0], [0.0, 2.0], [1.0, 0.0], [-1.0, 0.25]])
+        grad = np.zeros((R, 4))
+        L.check(lib.lgv_ensemble_diff_backward(e, L.ptr(w), L.ptr(grad)), "ensemble_diff_backward")
+        c = C.c_uint64()
+        L.check(lib.lgv_ensemble_get_counter(e, C.byref(c)), "get_counter")
+        assert c.value == 9 + S
+        for r, sp in enumerate(specs):
+            lat = EmLattice(lgv, sp["N"], seed=sp["seed"], mass0=sp["mass0"], lam=sp["lam"], H=sp["H"],
+                            gamma=sp["gamma"], dmassdt=-0.2)
+            lat.set_state(states[r])
+            lat.counter(9)
+            o1 = lat.forward(dt, S, b, K, t=t0)
+            g1 = lat.backward(w[r])
+            fin = np.empty((sp["N"],) * 3 + (10,))
+            L.check(lib.lgv_ensemble_get_state(e, r, L.ptr(fin)), "get_state")
+            assert np.array_equal(fin, lat.get_state()), f"replica {r}: final state differs"
+            np.testing.assert_allclose(obs[r], o1, rtol=1e-13, atol=1e-15)
+            assert_grad_close(grad[r], g1, 1e-12, f"ensemble replica {r}")
+            lat.close()
+    finally:
+        lib.lgv_ensemble_destroy(e)
