@@ -142,7 +142,7 @@ def cpu_reference_rate(N, scounts, seconds=15.0, steps=None, warmup=1):
 
 
 def run_reference(a):
-    rank = int(os.environ.get("RANK", "0"))
+    _, rank, _ = rank_env()
     if rank != 0:
         return 0
     scounts = tuple(int(x) for x in a.scounts.split(","))
@@ -405,15 +405,40 @@ def run_adjoint_batch(reps=3):
     }
 
 
+def rank_env():
+    """(world, rank, local rank) from the torchrun environment (1, 0, 0 without it)."""
+    return (int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def replica_seed(base, rank):
+    """Each rank advances its own replica: the lattice does not shard."""
+    return base + rank
+
+
+def max_over_ranks(x, dist, device):
+    """The slowest rank's time (every rank calls this at the same point)."""
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(units_per_rank, world, seconds):
+    """Units processed by all ranks per second of the slowest rank."""
+    return units_per_rank * world / seconds
+
+
 def run_ours(a):
     import ctypes as C
 
     import numpy as np
     import torch
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world, rank, local = rank_env()
     torch.cuda.set_device(local)
     dist = None
     if world > 1:
@@ -430,7 +455,7 @@ def run_ours(a):
     name = "PV2HBSplit%d%d" % scounts
     N = a.N
     V = N ** 3
-    p = L.make_params(N, seed=a.seed + rank, **COEF)
+    p = L.make_params(N, seed=replica_seed(a.seed, rank), **COEF)
     h = C.c_void_p()
     L.check(lib.lgv_create(C.byref(p), C.byref(h)), "lgv_create")
     stream = torch.cuda.Stream()
@@ -469,11 +494,7 @@ def run_ours(a):
     if dist:
         dist.barrier()
     ck = clocks.stop()
-    ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(e0.elapsed_time(e1), dist, "cuda")
     kern = {}
     for k, c in KCLASS.items():
         tot, n = C.c_double(), C.c_int64()
@@ -485,7 +506,7 @@ def run_ours(a):
     for k, (tot, n) in kern.items():
         launches += n * (5 if k == "measure" else 1)
 
-    value = V * a.steps * world / (ms / 1e3)
+    value = whole_job_rate(V * a.steps, world, ms / 1e3)
     peak, peak_kind = peaks()
     dom = max((k for k in ALG_BYTES if kern[k][1] > 0), key=lambda k: kern[k][0])
     tot, n = kern[dom]
@@ -526,13 +547,9 @@ def run_ours(a):
             L.check(lib.lgv_step(h, L.PV2HBSPLIT, scounts[0], scounts[1], DT, ts, 1), "step")
             ts += DT
         L.check(lib.lgv_get_state(h, C.c_void_p(u_host.data_ptr())), "get_state")
-        el = time.perf_counter() - t0
-        if dist:
-            t = torch.tensor([el], dtype=torch.float64, device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            el = float(t.item())
+        el = max_over_ranks(time.perf_counter() - t0, dist, "cuda")
         mbytes = msize * 8
-        e2e = {"value": V * a.steps * world / el, "unit": "site-updates/s",
+        e2e = {"value": whole_job_rate(V * a.steps, world, el), "unit": "site-updates/s",
                "h2d_bytes_per_step": 80 * V / a.steps,
                "d2h_bytes_per_step": (80 * V + n_meas * mbytes) / a.steps,
                "what": "lgv_set_state from pinned host AoS, K x lgv_step with lgv_measure to host every 10 steps, "
