@@ -134,6 +134,14 @@ int ensure(double **p, size_t n) {
   return LGV_OK;
 }
 
+// A bounded device wait (TMA completion) that gave up leaves a count behind:
+// report it once as an error.
+int check_waits() {
+  const unsigned n = lgv::read_wait_timeouts(true);
+  if (n) return fail(LGV_ERR_CUDA, "%u bounded device waits timed out (TMA copies did not complete)", n);
+  return LGV_OK;
+}
+
 int ensure_scratch(lgv_handle *h, size_t n) {
   if (h->scratch && h->scratch_len >= n) return LGV_OK;
   if (h->scratch) cudaFree(h->scratch);
@@ -502,7 +510,7 @@ int lgv_get_state(lgv_handle *h, double *host_aos) {
   LGV_CK(lgv::launch_rb_to_aos(h->cur, h->staging, h->N, h->stream));
   LGV_CK(cudaMemcpyAsync(host_aos, h->staging, 10 * h->V * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   LGV_CK(cudaStreamSynchronize(h->stream));
-  return LGV_OK;
+  return check_waits();
 }
 
 int lgv_set_state_device(lgv_handle *h, const double *dev_aos) {
@@ -700,7 +708,7 @@ int lgv_synchronize(lgv_handle *h) {
   if (!h) return fail(LGV_ERR_INVALID, "handle is NULL");
   DeviceGuard g(h->device);
   LGV_CK(cudaStreamSynchronize(h->stream));
-  return LGV_OK;
+  return check_waits();
 }
 
 int lgv_timing_enable(lgv_handle *h, int enable) {

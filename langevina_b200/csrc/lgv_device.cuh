@@ -101,12 +101,16 @@ __device__ __forceinline__ void box_muller(uint64_t ra, uint64_t rb, double &z0,
 }
 
 // O(4) algebra (O4AlgebraHelper.h:17-97) ------------------------------------
-// expmul(v) = (cos|v|, -sin|v|/|v| * v).  For |v|^2 <= 1/16 the cosine and
-// sin(x)/x come from their Maclaurin series in x^2 (terms through x^12 keep
-// the truncation below 1e-17 relative); larger angles use sincos().  Below
+// expmul(v) = (cos|v|, -sin|v|/|v| * v).  The cosine and sin(x)/x come from
+// their Maclaurin series in x^2: through x^6 for |v|^2 <= 1e-4 (the first
+// omitted terms, x^8/8! and x^8/9!, stay below 3e-21) and through x^12 for
+// |v|^2 <= 1/16 (below 1e-17 relative); larger angles use sincos().  Below
 // |v| = 1e-20 the identity is returned, as in the reference.
 __device__ __forceinline__ void cos_sinc(double x2, double &c, double &sc) {
-  if (x2 <= 0.0625) {
+  if (x2 <= 1e-4) {
+    c = fma(fma(fma(-1.0 / 720.0, x2, 1.0 / 24.0), x2, -0.5), x2, 1.0);
+    sc = fma(fma(fma(-1.0 / 5040.0, x2, 1.0 / 120.0), x2, -1.0 / 6.0), x2, 1.0);
+  } else if (x2 <= 0.0625) {
     // cos x = sum (-1)^n x^2n/(2n)!,  sin x / x = sum (-1)^n x^2n/(2n+1)!
     c = 1.0 / 479001600.0;                 // 1/12!
     c = fma(c, -x2, 1.0 / 3628800.0);      // 1/10!

@@ -1,0 +1,321 @@
+// lgv_ideal_tma.cu -- the fused ideal step (IdealPV2::step_no_reject,
+// Stepper.cxx:68-176) with its tiles staged by the Tensor Memory Accelerator.
+//
+// A CTA of 256 threads owns a 32 x 8 column of sites and marches up a
+// z-chunk, as ideal_kernel does.  What changes is how a plane reaches shared
+// memory: the tile's own 256 sites of each of the 10 components are one TMA
+// box {16 m, 8 rows, 1 plane, 2 parity halves} of the red-black layout
+// (cp.async.bulk.tensor, completion on an mbarrier, issued by one thread),
+// and only the 84-site ring around the tile (periodic wrap) still comes by
+// per-thread cp.async.  Shared memory keeps the red-black order, and each
+// half warp owns the sites of one x-parity, so every shared-memory access of
+// a half warp is 16 consecutive doubles.
+//
+// Used for N divisible by 32 (whole tiles; TMA strides need N/2 even); other
+// sizes and the batched ensembles use ideal_kernel.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+
+#include <map>
+#include <mutex>
+#include <utility>
+
+#include "lgv_internal.h"
+
+namespace lgv {
+
+// bounded waits that gave up (read and cleared by the host)
+__device__ unsigned g_wait_timeouts = 0;
+
+namespace {
+
+constexpr int TX = 32, TY = 8, NT = TX * TY;
+constexpr int HM = TX / 2;                    // m per half row of the tile
+constexpr int CORE = 2 * TY * HM;             // doubles per component per plane (both halves)
+constexpr int NHALO = 2 * (TX + 2) + 2 * TY;  // ring sites
+constexpr int PM = HM + 2;                    // m slots per padded phi' half row
+constexpr int PR = TY + 2;                    // padded rows
+constexpr int PH = 2 * PR * PM;               // doubles per padded phi' component plane
+constexpr unsigned kBoxBytes = CORE * 8;
+constexpr unsigned kPlaneBytes = 10 * kBoxBytes;
+// dynamic shared memory (doubles): core [2][10][CORE], ring [2][10][NHALO], phi' [3][4][PH]
+constexpr size_t kCoreOff = 0, kHaloOff = 2 * 10 * CORE, kPhiOff = kHaloOff + 2 * 10 * NHALO;
+constexpr size_t kSmemBytes = (kPhiOff + 3 * 4 * PH) * sizeof(double) + 128;  // + alignment slack
+static_assert(NHALO <= NT, "ring larger than the CTA");
+static_assert((kBoxBytes % 128) == 0, "TMA boxes stay 128-byte aligned");
+
+struct TmaMaps {
+  CUtensorMap m[10];
+};
+
+__device__ __forceinline__ int wrapn(int a, int n) {
+  a %= n;
+  return a < 0 ? a + n : a;
+}
+
+__device__ __forceinline__ unsigned smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void cp_async8(double *smem, const double *gmem) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_addr(smem)), "l"(gmem) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(unsigned bar, unsigned parity) {
+  unsigned done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(done)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+
+// Bounded wait for the phase `parity` of an mbarrier: false (and a count in
+// g_wait_timeouts) when it gives up.
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
+  for (int i = 0; i < (1 << 22); ++i)
+    if (mbar_try(bar, parity)) return true;
+  atomicAdd(&g_wait_timeouts, 1u);
+  return false;
+}
+
+// One thread: the 10 component boxes of plane k into core stage `dst`.
+__device__ __forceinline__ void issue_plane(const TmaMaps &maps, double *dst, unsigned bar, int m0, int j0, int k) {
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(kPlaneBytes) : "memory");
+#pragma unroll
+  for (int c = 0; c < 10; ++c) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+        "[%6];\n" ::"r"(smem_addr(dst + c * CORE)),
+        "l"(&maps.m[c]), "r"(m0), "r"(j0), "r"(k), "r"(0), "r"(bar)
+        : "memory");
+  }
+}
+
+__global__ void __launch_bounds__(NT, 2)
+    ideal_tma_kernel(const __grid_constant__ TmaMaps maps, Fields in, Fields out, Geo g, int zchunk, IdealArgs a) {
+  extern __shared__ __align__(128) double smem_raw[];
+  __shared__ __align__(8) unsigned long long mbar[2];
+  __shared__ int s_abort;
+  // TMA destinations must be 128-byte aligned: align the base explicitly
+  double *smem = smem_raw + ((128 - (smem_addr(smem_raw) & 127)) & 127) / sizeof(double);
+  double *core = smem + kCoreOff;
+  double *halo = smem + kHaloOff;
+  double *phs = smem + kPhiOff;
+  const int N = g.N;
+  const int tid = threadIdx.x;
+  const int ty = tid >> 5, hw = (tid >> 4) & 1, t = tid & 15;
+  const int lx = 2 * t + hw;  // each half warp owns one x-parity of the row
+  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+  const int z0 = blockIdx.z * zchunk;
+  const int z1 = min(z0 + zchunk, N);
+  const int nit = (z1 - z0) + 2;
+  const int xi = x0 + lx, yj = y0 + ty;
+  const unsigned bar0 = smem_addr(&mbar[0]), bar1 = smem_addr(&mbar[1]);
+
+  // ring site of this thread: padded coordinates (hx, hy), global (hxg, hyg)
+  int hx = 0, hy = 0, hxg = 0, hyg = 0;
+  const bool ring = tid < NHALO;
+  if (ring) {
+    const int h = tid;
+    if (h < TX + 2) { hx = h; hy = 0; }
+    else if (h < 2 * (TX + 2)) { hx = h - (TX + 2); hy = PR - 1; }
+    else if (h < 2 * (TX + 2) + TY) { hx = 0; hy = 1 + (h - 2 * (TX + 2)); }
+    else { hx = TX + 1; hy = 1 + (h - 2 * (TX + 2) - TY); }
+    hxg = wrapn(x0 - 1 + hx, N);
+    hyg = wrapn(y0 - 1 + hy, N);
+  }
+
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar0) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar1) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    s_abort = 0;
+  }
+  __syncthreads();
+  if (tid == 0) issue_plane(maps, core, bar0, x0 / 2, y0, wrapn(z0 - 1, N));  // plane z0-1: no ring needed
+
+  double pm[4], pc[4], pn[4], qc[6], qn[6];
+  unsigned wbar = bar0, wpar = 0;  // the barrier phase waited on last
+  for (int it = 0; it < nit; ++it) {
+    const int p = wrapn(z0 - 1 + it, N);
+    const int st = it & 1;
+    wbar = st ? bar1 : bar0;
+    wpar = (unsigned)((it >> 1) & 1);
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    if (!mbar_wait(wbar, wpar)) s_abort = 1;
+    __syncthreads();
+    if (s_abort) break;
+    if (it + 1 < nit) {
+      const int pnx = wrapn(p + 1, N), sn = st ^ 1;
+      if (tid == 0) issue_plane(maps, core + sn * 10 * CORE, sn ? bar1 : bar0, x0 / 2, y0, pnx);
+      if (ring) {
+        const long long oh = rb_off(g, hxg, hyg, pnx);
+#pragma unroll
+        for (int c = 0; c < 10; ++c) cp_async8(&halo[(sn * 10 + c) * NHALO + tid], in.c[c] + oh);
+      }
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+
+    const double *cr = core + st * 10 * CORE;
+    double *ph = phs + (it % 3) * 4 * PH;
+    // own site of plane p: half, core and padded phi' positions
+    const int hp = (hw + y0 + ty + p) & 1;
+    const int co = (hp * TY + ty) * HM + t;
+    const int po = (hp * PR + ty + 1) * PM + t + 1;
+#pragma unroll
+    for (int l = 0; l < 4; ++l) pn[l] = cr[l * CORE + co];
+#pragma unroll
+    for (int s = 0; s < 6; ++s) qn[s] = cr[(4 + s) * CORE + co];
+    rotate_site(pn, qn, a.dto2chi);
+#pragma unroll
+    for (int l = 0; l < 4; ++l) ph[l * PH + po] = pn[l];
+    if (ring && it >= 1) {
+      const double *hr = halo + st * 10 * NHALO;
+      double phh[4], qh[6];
+#pragma unroll
+      for (int l = 0; l < 4; ++l) phh[l] = hr[l * NHALO + tid];
+#pragma unroll
+      for (int s = 0; s < 6; ++s) qh[s] = hr[(4 + s) * NHALO + tid];
+      rotate_site(phh, qh, a.dto2chi);
+      const int lxh = hx - 1, lyh = hy - 1;
+      const int hh = (lxh + y0 + lyh + p) & 1;
+      const int pho = (hh * PR + hy) * PM + ((lxh + 2) >> 1);
+#pragma unroll
+      for (int l = 0; l < 4; ++l) ph[l * PH + pho] = phh[l];
+    }
+
+    if (it >= 2) {
+      const double *pp = phs + ((it + 2) % 3) * 4 * PH;  // phi' of plane p-1 (written last iteration)
+      const int kk = wrapn(p - 1, N);
+      const int nh = ((hw + y0 + ty + kk) & 1) ^ 1;  // the neighbours' half
+      const int rx = (nh * PR + ty + 1) * PM;
+      const int oxp = rx + t + 1 + hw, oxm = rx + t + hw;
+      const int oyp = (nh * PR + ty + 2) * PM + t + 1, oym = (nh * PR + ty) * PM + t + 1;
+      double xp[4], xm[4], yp[4], ym[4];
+#pragma unroll
+      for (int l = 0; l < 4; ++l) {
+        xp[l] = pp[l * PH + oxp];
+        xm[l] = pp[l * PH + oxm];
+        yp[l] = pp[l * PH + oyp];
+        ym[l] = pp[l * PH + oym];
+      }
+      const double *c = pc, *zp = pn, *zm = pm;
+      // axial charges (Stepper.cxx:112-133)
+#pragma unroll
+      for (int l = 0; l < 3; ++l) {
+        const double bx = -xp[0] * c[l + 1] + c[0] * xp[l + 1] + c[0] * xm[l + 1] - xm[0] * c[l + 1];
+        const double by = -yp[0] * c[l + 1] + c[0] * yp[l + 1] + c[0] * ym[l + 1] - ym[0] * c[l + 1];
+        const double bz = -zp[0] * c[l + 1] + c[0] * zp[l + 1] + c[0] * zm[l + 1] - zm[0] * c[l + 1];
+        qc[l] += a.dt * (bx * a.a2 + by * a.a2 + bz * a.a2 - a.H * c[l + 1]);
+      }
+      // vector charges, epsilon = +1 for the cyclic (s, s+1, s+2) (Stepper.cxx:135-163)
+#pragma unroll
+      for (int s = 0; s < 3; ++s) {
+        const int s1 = 1 + (s + 1) % 3, s2 = 1 + (s + 2) % 3;
+        const double bx = xp[s2] * c[s1] - c[s2] * xm[s1] - xp[s1] * c[s2] + c[s1] * xm[s2];
+        const double by = yp[s2] * c[s1] - c[s2] * ym[s1] - yp[s1] * c[s2] + c[s1] * ym[s2];
+        const double bz = zp[s2] * c[s1] - c[s2] * zm[s1] - zp[s1] * c[s2] + c[s1] * zm[s2];
+        qc[3 + s] += a.dt * (bx * a.a2 + by * a.a2 + bz * a.a2);
+      }
+      // second half rotation on a copy: pc (phi') stays the z-1 neighbour of the next plane
+      double pf[4] = {pc[0], pc[1], pc[2], pc[3]};
+      rotate_site(pf, qc, a.dto2chi);
+      const long long o = rb_off(g, xi, yj, kk);
+#pragma unroll
+      for (int l = 0; l < 4; ++l) out.c[l][o] = pf[l];
+#pragma unroll
+      for (int s = 0; s < 6; ++s) out.c[4 + s][o] = qc[s];
+    }
+#pragma unroll
+    for (int l = 0; l < 4; ++l) {
+      pm[l] = pc[l];
+      pc[l] = pn[l];
+    }
+#pragma unroll
+    for (int s = 0; s < 6; ++s) qc[s] = qn[s];
+  }
+  if (s_abort) {
+    // the plane that timed out may still be in flight: one more bounded wait before the CTA retires
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    if (tid == 0) mbar_wait(wbar, wpar);
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Tensor maps: one per component plane, 4-D view (m, j, k, half) of the
+// red-black layout; cached by (plane address, N).
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+bool plane_map(const double *plane, int N, CUtensorMap *out) {
+  static std::mutex mu;
+  static std::map<std::pair<const double *, int>, CUtensorMap> cache;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = cache.find({plane, N});
+  if (it != cache.end()) {
+    *out = it->second;
+    return true;
+  }
+  auto fn = encode_fn();
+  if (!fn) return false;
+  const cuuint64_t H = (cuuint64_t)(N / 2);
+  const cuuint64_t dims[4] = {H, (cuuint64_t)N, (cuuint64_t)N, 2};
+  const cuuint64_t strides[3] = {H * 8, (cuuint64_t)N * H * 8, (cuuint64_t)N * N * H * 8};
+  const cuuint32_t box[4] = {HM, TY, 1, 2};
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  CUtensorMap m;
+  if (fn(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<double *>(plane), dims, strides, box, estr,
+         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return false;
+  if (cache.size() > 4096) cache.clear();
+  cache.emplace(std::make_pair(plane, N), m);
+  *out = m;
+  return true;
+}
+
+}  // namespace
+
+bool ideal_tma_supported(int N) {
+  return N >= 32 && N % 32 == 0 && encode_fn() != nullptr;
+}
+
+cudaError_t launch_ideal_tma(Fields in, Fields out, int N, int zchunk, const IdealArgs &a, cudaStream_t st) {
+  if (!ideal_tma_supported(N)) return cudaErrorInvalidValue;
+  for (int c = 0; c < 10; ++c)
+    if (((uintptr_t)in.c[c] & 15) != 0) return cudaErrorMisalignedAddress;
+  TmaMaps maps;
+  for (int c = 0; c < 10; ++c)
+    if (!plane_map(in.c[c], N, &maps.m[c])) return cudaErrorInvalidValue;
+  cudaError_t e = cudaFuncSetAttribute(ideal_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
+  if (e != cudaSuccess) return e;
+  const Geo g = make_geo(N);
+  dim3 grid(N / TX, N / TY, (unsigned)((N + zchunk - 1) / zchunk));
+  ideal_tma_kernel<<<grid, NT, kSmemBytes, st>>>(maps, in, out, g, zchunk, a);
+  return cudaGetLastError();
+}
+
+unsigned read_wait_timeouts(bool clear) {
+  unsigned v = 0;
+  cudaMemcpyFromSymbol(&v, g_wait_timeouts, sizeof(v));
+  if (clear && v) {
+    const unsigned z = 0;
+    cudaMemcpyToSymbol(g_wait_timeouts, &z, sizeof(z));
+  }
+  return v;
+}
+
+}  // namespace lgv

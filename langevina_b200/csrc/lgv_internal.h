@@ -193,6 +193,11 @@ cudaError_t launch_charge_dir(Fields in, Fields out, int N, int dir, const Charg
                               bool *swapped);
 cudaError_t launch_em(Fields in, Fields out, int N, const EmArgs &a, cudaStream_t st);
 cudaError_t launch_ideal(Fields in, Fields out, int N, const IdealArgs &a, cudaStream_t st);
+// TMA-staged ideal step (lgv_ideal_tma.cu): N divisible by 32
+bool ideal_tma_supported(int N);
+cudaError_t launch_ideal_tma(Fields in, Fields out, int N, int zchunk, const IdealArgs &a, cudaStream_t st);
+// bounded device waits that gave up since the last clear
+unsigned read_wait_timeouts(bool clear);
 // energy: writes E into dev_out[0]; scratch >= energy_scratch_doubles(N)
 size_t energy_scratch_doubles(int N);
 cudaError_t launch_energy(Fields f, int N, double H, double inv2chi_half, double *scratch, double *dev_out,

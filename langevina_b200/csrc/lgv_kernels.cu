@@ -18,6 +18,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 
 namespace lgv {
 
@@ -2069,6 +2070,11 @@ cudaError_t launch_ideal(Fields in, Fields out, int N, const IdealArgs &a, cudaS
   if (zc > 32) zc = 32;
   if (zc < 4) zc = 4;
   if (zc > N) zc = N;
+  static const bool tma_off = [] {
+    const char *v = std::getenv("LGV_IDEAL_TMA");
+    return v && v[0] == '0';
+  }();
+  if (!tma_off && ideal_tma_supported(N)) return launch_ideal_tma(in, out, N, (int)zc, a, st);
   dim3 grid((N + TX - 1) / TX, (N + TY - 1) / TY, (unsigned)((N + zc - 1) / zc));
   cudaError_t e = allow_smem(ideal_kernel<TX, TY>, T::SMEM);
   if (e != cudaSuccess) return e;

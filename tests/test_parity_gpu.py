@@ -106,9 +106,11 @@ def test_charge_heatbath_counter(lgv, oracle_mod, N):
 
 
 @pytest.mark.parametrize("N,dt,chi", [(4, 0.04, 5.0), (6, 0.04, 5.0), (8, 0.2, 5.0), (16, 0.04, 5.0),
-                                      (34, 0.04, 5.0), (48, 0.01, 5.0), (8, 0.5, 0.2)])
+                                      (34, 0.04, 5.0), (48, 0.01, 5.0), (8, 0.5, 0.2), (32, 0.04, 5.0),
+                                      (64, 0.04, 5.0), (32, 0.5, 0.2), (96, 0.02, 5.0)])
 def test_ideal_step(lgv, oracle_mod, N, dt, chi):
-    """dt=0.5, chi=0.2 drives half-step angles past 1/4: the sincos branch."""
+    """dt=0.5, chi=0.2 drives half-step angles past 1/4: the sincos branch.
+    N divisible by 32 runs the TMA-staged kernel, other N the cp.async one."""
     g, o = pair(lgv, oracle_mod, N, oracle_mod.COUNTER, chi=chi)
     u = rand_state(N, 31, chi=chi)
     g.set_state(u)
@@ -142,7 +144,7 @@ def test_em_injected_and_counter(lgv, oracle_mod, N):
 
 
 @pytest.mark.parametrize("ev,inner,outer,N", [(PV2, 2, 3, 8), (PV2, 1, 1, 8), (PV2, 2, 3, 16), (NODIFF, 2, 3, 6),
-                                              (ONLYDIFF, 2, 3, 6), (PV2, 3, 1, 4)])
+                                              (ONLYDIFF, 2, 3, 6), (PV2, 3, 1, 4), (PV2, 2, 3, 32)])
 def test_pv2hbsplit_counter(lgv, oracle_mod, ev, inner, outer, N):
     g, o = pair(lgv, oracle_mod, N, oracle_mod.COUNTER)
     u = rand_state(N, 51)
