@@ -430,6 +430,8 @@ int lgv_create(const lgv_params *params, lgv_handle **out) {
   {
     const char *f = std::getenv("LGV_HB_FUSED");
     h->hb_fused = f && f[0] == '1';
+    // one face per launch (the faster path on B200); LGV_CHARGE_FUSED=1 selects
+    // both faces of a direction per launch
     const char *c = std::getenv("LGV_CHARGE_FUSED");
     h->charge_per_face = !(c && c[0] == '1');
   }

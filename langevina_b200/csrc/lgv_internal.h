@@ -189,6 +189,8 @@ cudaError_t launch_charge_pass(Fields f, int N, int dir, int eoA, const ChargeAr
 // Both faces of direction dir.  x runs in place on `in`; y and z read `in`
 // and write the charges of `out` (*swapped = true: the caller swaps the
 // charge planes).
+// shared-memory slab kernel for both faces of a direction (N divisible by 32)
+bool charge_slab_supported(int N);
 cudaError_t launch_charge_dir(Fields in, Fields out, int N, int dir, const ChargeDirPair &p, cudaStream_t st,
                               bool *swapped);
 cudaError_t launch_em(Fields in, Fields out, int N, const EmArgs &a, cudaStream_t st);

@@ -238,6 +238,10 @@ __device__ __forceinline__ void cp_async8(double *smem, const double *gmem) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
 }
+__device__ __forceinline__ void cp_async16(double *smem, const double *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
@@ -756,6 +760,144 @@ __global__ void __launch_bounds__(128) charge_line_kernel(Fields in, Fields out,
       tm1 = tw; jm1 = j; km1 = k;
     }
     (void)tm2;
+  }
+  if (MON) mon_flush(mon, a.mon);
+}
+
+// ----------------------------------------------------------------------------
+// Both faces of one charge direction per launch, staged in shared memory.
+// The CTA copies its slab of the six charge planes to shared memory with
+// coalesced half-row loads, applies every link of the first face, then every
+// link of the second, and writes the slab back: the two faces cost one read
+// and one write of the charges instead of two of each.
+//   x (DIR 0): the slab is `nrows` whole rows (no halo: x links stay in a row).
+//   y, z (DIR 1, 2): 32 natural columns (16 elements of each parity half-row)
+//   along a segment [s0, s1) of the line at fixed k (y) or j (z), plus two
+//   sites either side; halo links are recomputed bit for bit, only links whose
+//   A site lies in the segment count in monitors and flags, and only segment
+//   sites are written, so the kernel reads `in` and writes `out`.
+// Links are the same charge_link updates, streams and order as the per-face
+// kernels (Stepper.cxx:471-518).
+constexpr int kSlabThreads = 256;
+
+template <int DIR, bool INJECTED, bool MON>
+__global__ void __launch_bounds__(kSlabThreads) charge_slab_kernel(Fields in, Fields out, Geo g, ChargeDirArgs a,
+                                                                   int seglen, int nrows) {
+  extern __shared__ double S[];
+  const int N = g.N, H = g.H;
+  const long long V2 = g.V2, V = 2 * V2;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  MonLocal mon;
+  if (DIR == 0) {
+    const long long R0 = (long long)blockIdx.x * nrows;
+    const int nr = (int)min((long long)nrows, (long long)N * N - R0);
+    // S[L][r][h][m]
+    // 16-byte cp.async: every load of the slab in flight at once
+    const int HC = H / 2;  // 16-byte chunks per half row
+#pragma unroll
+    for (int L = 0; L < 6; ++L)  // static component index: Fields stays in the parameter space
+      for (int e = tid; e < nr * H; e += kSlabThreads) {
+        const int r = e / H, cc = e - r * H;
+        const int h = cc >= HC ? 1 : 0, m = 2 * (cc - h * HC);
+        cp_async16(&S[((L * nrows + r) * 2 + h) * H + m], in.c[4 + L] + h * V2 + (R0 + r) * H + m);
+      }
+    cp_async_commit();
+    cp_async_wait_all();
+    __syncthreads();
+#pragma unroll
+    for (int pi = 0; pi < 2; ++pi) {  // static face index: the arguments stay in the parameter space
+      const int eo = a.eo[pi];
+      for (int e = tid; e < nr * H; e += kSlabThreads) {
+        const int r = e / H, u = e - r * H;
+        const long long R = R0 + r;
+        const int j = (int)(R % N), k = (int)(R / N);
+        const int sA = (eo + j + k) & 1;  // A sites at i = 2u + sA
+        {
+          const int iA = 2 * u + sA;
+          const int iB = (iA + 1 == N) ? 0 : iA + 1;
+          double *pa = S + ((size_t)r * 2 + eo) * H + u;
+          double *pb = S + ((size_t)r * 2 + (eo ^ 1)) * H + (iB >> 1);
+          const size_t ls = (size_t)nrows * 2 * H;
+          double nA[6], nB[6];
+#pragma unroll
+          for (int L = 0; L < 6; ++L) {
+            nA[L] = pa[L * ls];
+            nB[L] = pb[L * ls];
+          }
+          charge_link<INJECTED, MON>(nA, nB, a, pi, R * N + iA, V, true, mon);
+#pragma unroll
+          for (int L = 0; L < 6; ++L) {
+            pa[L * ls] = nA[L];
+            pb[L * ls] = nB[L];
+          }
+        }
+      }
+      __syncthreads();
+    }
+#pragma unroll
+    for (int L = 0; L < 6; ++L)
+      for (int r = 0; r < nr; ++r)
+        for (int e = tid; e < 2 * H; e += kSlabThreads) {
+          const int h = e >= H ? 1 : 0, m = e - h * H;
+          out.c[4 + L][h * V2 + (R0 + r) * H + m] = S[((L * nrows + r) * 2 + h) * H + m];
+        }
+  } else {
+    const int x0 = blockIdx.x * 32, m0 = x0 >> 1;
+    const int c2 = blockIdx.y;  // k for y lines, j for z lines
+    const int s0 = blockIdx.z * seglen, s1 = min(s0 + seglen, N);
+    const int W = (s1 - s0) + 4;  // window positions t = s0 - 2 + w
+    // S[L][w][h][mm]: 32 doubles per (L, w)
+    const int h = lane >> 4, mm = lane & 15;
+    // 16-byte cp.async: every load of the slab in flight at once
+#pragma unroll
+    for (int L = 0; L < 6; ++L)
+      for (int e = tid; e < W * 16; e += kSlabThreads) {
+        const int w = e >> 4, cc = e & 15;
+        const int hc = cc >> 3, mc = 2 * (cc & 7);
+        const int t = wrapn(s0 - 2 + w, N);
+        const int j = DIR == 1 ? t : c2, k = DIR == 1 ? c2 : t;
+        cp_async16(&S[((L * W + w) * 2 + hc) * 16 + mc], in.c[4 + L] + hc * V2 + ((long long)k * N + j) * H + m0 + mc);
+      }
+    cp_async_commit();
+    cp_async_wait_all();
+    __syncthreads();
+    const size_t ls = (size_t)W * 32;
+    const int lx = lane;  // natural column x0 + lx
+#pragma unroll
+    for (int pi = 0; pi < 2; ++pi) {
+      const int eo = a.eo[pi];
+      const int w0 = (eo + lx + c2 + s0) & 1;  // A sites of this column at w = w0 + 2u
+      // first face: every link inside the window; second face: links with both ends in [1, W-2]
+      const int wlo = pi == 0 ? 0 : 1, whi = pi == 0 ? W - 1 : W - 2;
+      for (int w = w0 + 2 * warp; w + 1 <= whi; w += 2 * (kSlabThreads / 32)) {
+        if (w < wlo) continue;
+        const int tA = wrapn(s0 - 2 + w, N);
+        const int j = DIR == 1 ? tA : c2, k = DIR == 1 ? c2 : tA;
+        double *pa = S + ((size_t)w * 2 + eo) * 16 + (lx >> 1);
+        double *pb = S + ((size_t)(w + 1) * 2 + (eo ^ 1)) * 16 + (lx >> 1);
+        double nA[6], nB[6];
+#pragma unroll
+        for (int L = 0; L < 6; ++L) {
+          nA[L] = pa[L * ls];
+          nB[L] = pb[L * ls];
+        }
+        const bool own = (w - 2) >= 0 && (w - 2) < (s1 - s0);
+        charge_link<INJECTED, MON>(nA, nB, a, pi, ((long long)k * N + j) * N + x0 + lx, V, own, mon);
+#pragma unroll
+        for (int L = 0; L < 6; ++L) {
+          pa[L * ls] = nA[L];
+          pb[L * ls] = nB[L];
+        }
+      }
+      __syncthreads();
+    }
+#pragma unroll
+    for (int L = 0; L < 6; ++L)
+      for (int w = 2 + warp; w < W - 2; w += kSlabThreads / 32) {
+        const int t = s0 - 2 + w;
+        const int j = DIR == 1 ? t : c2, k = DIR == 1 ? c2 : t;
+        out.c[4 + L][h * V2 + ((long long)k * N + j) * H + m0 + mm] = S[(L * W + w) * 32 + lane];
+      }
   }
   if (MON) mon_flush(mon, a.mon);
 }
@@ -1979,6 +2121,8 @@ cudaError_t launch_charge_pass(Fields f, int N, int dir, int eoA, const ChargeAr
 
 static int charge_seglen(int N) { return N >= 64 ? 32 : N; }
 
+bool charge_slab_supported(int N) { return N >= 32 && N % 32 == 0 && N <= 2048; }
+
 cudaError_t launch_charge_dir(Fields in, Fields out, int N, int dir, const ChargeDirPair &p, cudaStream_t st,
                               bool *swapped) {
   const Geo g = make_geo(N);
@@ -1995,6 +2139,36 @@ cudaError_t launch_charge_dir(Fields in, Fields out, int N, int dir, const Charg
   a.flags = p.flags;
   a.mon = p.mon;
   const bool inj = a.q != nullptr, mon = a.mon != nullptr;
+  if (charge_slab_supported(N)) {
+    *swapped = true;
+    int sl = 0, nr = 0;
+    size_t sm = 0;
+    dim3 grid;
+    if (dir == 0) {
+      nr = (int)std::max(1, std::min(4, 512 / g.H));
+      sm = (size_t)6 * nr * 2 * g.H * sizeof(double);
+      grid = dim3((unsigned)(((long long)N * N + nr - 1) / nr));
+    } else {
+      sl = std::min(N, 32);
+      sm = (size_t)6 * (sl + 4) * 32 * sizeof(double);
+      grid = dim3(N / 32, N, (N + sl - 1) / sl);
+    }
+#define LGV_SLAB(D, I, M)                                                                   \
+  do {                                                                                      \
+    cudaError_t e_ = allow_smem(charge_slab_kernel<D, I, M>, sm);                           \
+    if (e_ != cudaSuccess) return e_;                                                       \
+    charge_slab_kernel<D, I, M><<<grid, kSlabThreads, sm, st>>>(in, out, g, a, sl, nr);     \
+  } while (0)
+#define LGV_SLAB_DIR(D) \
+  if (inj) { if (mon) LGV_SLAB(D, true, true); else LGV_SLAB(D, true, false); } \
+  else { if (mon) LGV_SLAB(D, false, true); else LGV_SLAB(D, false, false); }
+    if (dir == 0) { LGV_SLAB_DIR(0) }
+    else if (dir == 1) { LGV_SLAB_DIR(1) }
+    else { LGV_SLAB_DIR(2) }
+#undef LGV_SLAB_DIR
+#undef LGV_SLAB
+    return cudaGetLastError();
+  }
   if (dir == 0 && g.H > 256) {
     // rows longer than one 256-thread CTA: the two faces as separate launches
     *swapped = false;

@@ -317,12 +317,15 @@ def test_phi_heatbath_fused_sweep_variant(lgv, oracle_mod, N, mode, monkeypatch)
     assert_state_close(g.get_state(), o.get_state(), what="fused HB sweep")
 
 
-@pytest.mark.parametrize("N,seed,fused", [(64, 15, True), (66, 16, True), (8, 17, True), (66, 18, False)])
+@pytest.mark.parametrize("N,seed,fused", [(64, 15, True), (66, 16, True), (8, 17, True), (66, 18, False),
+                                          (32, 20, True), (64, 23, False), (96, 24, True)])
 def test_charge_heatbath_injected_segments_and_fused(lgv, oracle_mod, N, seed, fused, monkeypatch):
-    """LGV_CHARGE_FUSED=1 runs both faces of a direction per launch: x rows
-    per CTA, y and z streamed in 32-site segments with two-site halos for
-    N >= 64 (66 leaves a ragged last segment).  Both it and the default
-    single-face launches reproduce the oracle decision for decision."""
+    """LGV_CHARGE_FUSED=1 runs both faces of a direction per launch and
+    reproduces the oracle decision for decision: for N divisible by 32 the
+    shared-memory slab kernel (x: whole rows; y, z: 32-site segments with
+    two-site halos), otherwise x rows per CTA and y, z streamed in 32-site
+    segments (66 leaves a ragged last segment).  The default single-face
+    launches (fused=False) do too."""
     if fused:
         monkeypatch.setenv("LGV_CHARGE_FUSED", "1")
     g, o = pair(lgv, oracle_mod, N, oracle_mod.INJECTED)
@@ -346,8 +349,9 @@ def test_charge_heatbath_injected_segments_and_fused(lgv, oracle_mod, N, seed, f
         assert gm[k] == om[k], k
 
 
-@pytest.mark.parametrize("N", [64, 70])
+@pytest.mark.parametrize("N", [64, 70, 96, 160])
 def test_charge_heatbath_counter_segments(lgv, oracle_mod, N, monkeypatch):
+    """64, 96, 160: the slab kernel; 70: streamed lines with a ragged last segment."""
     monkeypatch.setenv("LGV_CHARGE_FUSED", "1")
     g, o = pair(lgv, oracle_mod, N, oracle_mod.COUNTER)
     monkeypatch.delenv("LGV_CHARGE_FUSED")
