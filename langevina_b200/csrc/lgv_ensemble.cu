@@ -65,7 +65,7 @@ struct lgv_ensemble {
   std::vector<double *> bufs;
   RepDesc *dd = nullptr;
   EnsDyn *dyn = nullptr;
-  BlockMap ideal_map, plane_map;
+  BlockMap ideal_map, plane_map, slab_map;
   double *partial = nullptr, *oavg = nullptr;
   cudaStream_t own = nullptr, stream = nullptr;
   int phase_phi = 0, phase_q = 0;
@@ -154,7 +154,7 @@ int build_map(lgv_ensemble *e, BlockMap &m, const std::vector<int> &blocks_per_r
 int configure(lgv_ensemble *e) {
   int tx = 32, ty = 8;
   lgv::ideal_tile_dims(e->tile, &tx, &ty);
-  std::vector<int> ib(e->R), pb(e->R);
+  std::vector<int> ib(e->R), pb(e->R), sb(e->R);
   for (int r = 0; r < e->R; ++r) {
     RepDesc &d = e->hd[r];
     const int N = d.g.N;
@@ -165,10 +165,12 @@ int configure(lgv_ensemble *e) {
     d.igz = (N + d.izc - 1) / d.izc;
     ib[r] = d.igx * d.igy * d.igz;
     pb[r] = d.nchunk * N;
+    sb[r] = d.nchunk * ((N + lgv::kBatchPlanes - 1) / lgv::kBatchPlanes);
   }
   ECK(cudaMemcpy(e->dd, e->hd.data(), e->R * sizeof(RepDesc), cudaMemcpyHostToDevice));
   ETRY(build_map(e, e->ideal_map, ib));
   ETRY(build_map(e, e->plane_map, pb));
+  ETRY(build_map(e, e->slab_map, sb));
   if (e->partial) cudaFree(e->partial);
   e->partial = nullptr;
   ECK(cudaMalloc((void **)&e->partial, (size_t)e->plane_map.nblocks * 11 * sizeof(double)));
@@ -193,7 +195,7 @@ int step_ctr(int ev, int inner, int outer) {
 
 // Enqueue one step on e->stream (also used inside graph capture).
 int enqueue_step(lgv_ensemble *e, int ev, int inner, int outer, double dt) {
-  const int nb_i = e->ideal_map.nblocks, nb_p = e->plane_map.nblocks;
+  const int nb_i = e->ideal_map.nblocks, nb_p = e->plane_map.nblocks, nb_s = e->slab_map.nblocks;
   int off = 0;
   auto ideal = [&](double d) -> int {
     ECK(lgv::launch_batch_ideal(e->dd, e->ideal_map.rep, e->ideal_map.first, nb_i, e->tile, e->phase_phi,
@@ -205,14 +207,14 @@ int enqueue_step(lgv_ensemble *e, int ev, int inner, int outer, double dt) {
   };
   auto hb = [&](double d) -> int {
     for (int parity = 0; parity < 2; ++parity)
-      ECK(lgv::launch_batch_hb(e->dd, e->dyn, e->plane_map.rep, e->plane_map.first, nb_p, e->phase_phi, parity, d, off,
+      ECK(lgv::launch_batch_hb(e->dd, e->dyn, e->slab_map.rep, e->slab_map.first, nb_s, e->phase_phi, parity, d, off,
                                e->stream));
     off += 1;
     return LGV_OK;
   };
   auto charge = [&](double d) -> int {
     for (int pass = 0; pass < 6; ++pass)
-      ECK(lgv::launch_batch_charge(e->dd, e->dyn, e->plane_map.rep, e->plane_map.first, nb_p, e->phase_q, pass, d,
+      ECK(lgv::launch_batch_charge(e->dd, e->dyn, e->slab_map.rep, e->slab_map.first, nb_s, e->phase_q, pass, d,
                                    off, e->stream));
     off += 7;
     return LGV_OK;
@@ -324,6 +326,7 @@ int lgv_ensemble_destroy(lgv_ensemble *e) {
   for (double *b : e->bufs) cudaFree(b);
   free_map(e->ideal_map);
   free_map(e->plane_map);
+  free_map(e->slab_map);
   if (e->dd) cudaFree(e->dd);
   if (e->dyn) cudaFree(e->dyn);
   if (e->partial) cudaFree(e->partial);

@@ -39,9 +39,15 @@ constexpr int PR = TY + 2;                    // padded rows
 constexpr int PH = 2 * PR * PM;               // doubles per padded phi' component plane
 constexpr unsigned kBoxBytes = CORE * 8;
 constexpr unsigned kPlaneBytes = 10 * kBoxBytes;
-// dynamic shared memory (doubles): core [2][10][CORE], ring [2][10][NHALO], phi' [3][4][PH]
-constexpr size_t kCoreOff = 0, kHaloOff = 2 * 10 * CORE, kPhiOff = kHaloOff + 2 * 10 * NHALO;
-constexpr size_t kSmemBytes = (kPhiOff + 3 * 4 * PH) * sizeof(double) + 128;  // + alignment slack
+// Two pipeline stages: plane p is consumed while plane p+1 loads.  (A third
+// stage, prefetching p+2, measured slower on B200: 0.88 against 0.67 ms per
+// 256^3 launch, with more barrier and MIO stalls.)
+constexpr int NS = 2;
+// dynamic shared memory (doubles): core [NS][10][CORE], ring [NS][10][NHALO], phi' [2][4][PH];
+// offsets rounded to 16 doubles (128-byte shared-memory wavefronts)
+constexpr size_t round16(size_t n) { return (n + 15) / 16 * 16; }
+constexpr size_t kCoreOff = 0, kHaloOff = NS * 10 * CORE, kPhiOff = round16(kHaloOff + NS * 10 * NHALO);
+constexpr size_t kSmemBytes = (kPhiOff + 2 * 4 * PH) * sizeof(double) + 128;  // + alignment slack
 static_assert(NHALO <= NT, "ring larger than the CTA");
 static_assert((kBoxBytes % 128) == 0, "TMA boxes stay 128-byte aligned");
 
@@ -96,7 +102,7 @@ __device__ __forceinline__ void issue_plane(const TmaMaps &maps, double *dst, un
 __global__ void __launch_bounds__(NT, 2)
     ideal_tma_kernel(const __grid_constant__ TmaMaps maps, Fields in, Fields out, Geo g, int zchunk, IdealArgs a) {
   extern __shared__ __align__(128) double smem_raw[];
-  __shared__ __align__(8) unsigned long long mbar[2];
+  __shared__ __align__(8) unsigned long long mbar[NS];
   __shared__ int s_abort;
   // TMA destinations must be 128-byte aligned: align the base explicitly
   double *smem = smem_raw + ((128 - (smem_addr(smem_raw) & 127)) & 127) / sizeof(double);
@@ -112,7 +118,7 @@ __global__ void __launch_bounds__(NT, 2)
   const int z1 = min(z0 + zchunk, N);
   const int nit = (z1 - z0) + 2;
   const int xi = x0 + lx, yj = y0 + ty;
-  const unsigned bar0 = smem_addr(&mbar[0]), bar1 = smem_addr(&mbar[1]);
+  const unsigned bar0 = smem_addr(&mbar[0]);  // stage s uses bar0 + 8 s
 
   // ring site of this thread: padded coordinates (hx, hy), global (hxg, hyg)
   int hx = 0, hy = 0, hxg = 0, hyg = 0;
@@ -128,38 +134,44 @@ __global__ void __launch_bounds__(NT, 2)
   }
 
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar0) : "memory");
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar1) : "memory");
+    for (int s = 0; s < NS; ++s) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar0 + 8 * s) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     s_abort = 0;
   }
   __syncthreads();
-  if (tid == 0) issue_plane(maps, core, bar0, x0 / 2, y0, wrapn(z0 - 1, N));  // plane z0-1: no ring needed
+  // Plane q of the march (q = 0 is z0-1, which feeds only the own column's
+  // z-1 neighbour and needs no ring) goes to stage q % NS; one cp.async group
+  // per plane, possibly empty, so waiting for all groups covers plane q.
+  auto issue = [&](int q) {
+    const int pl = wrapn(z0 - 1 + q, N), sn = q % NS;
+    if (tid == 0) issue_plane(maps, core + sn * 10 * CORE, bar0 + 8 * sn, x0 / 2, y0, pl);
+    if (ring && q >= 1) {
+      const long long oh = rb_off(g, hxg, hyg, pl);
+#pragma unroll
+      for (int c = 0; c < 10; ++c) cp_async8(&halo[(sn * 10 + c) * NHALO + tid], in.c[c] + oh);
+    }
+  };
+  for (int q = 0; q < NS - 1; ++q) {  // nit >= 3 >= NS - 1
+    issue(q);
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  }
 
   double pm[4], pc[4], pn[4], qc[6], qn[6];
   unsigned wbar = bar0, wpar = 0;  // the barrier phase waited on last
   for (int it = 0; it < nit; ++it) {
     const int p = wrapn(z0 - 1 + it, N);
-    const int st = it & 1;
-    wbar = st ? bar1 : bar0;
-    wpar = (unsigned)((it >> 1) & 1);
+    const int st = it % NS;
+    wbar = bar0 + 8 * st;
+    wpar = (unsigned)((it / NS) & 1);
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     if (!mbar_wait(wbar, wpar)) s_abort = 1;
     __syncthreads();
     if (s_abort) break;
-    if (it + 1 < nit) {
-      const int pnx = wrapn(p + 1, N), sn = st ^ 1;
-      if (tid == 0) issue_plane(maps, core + sn * 10 * CORE, sn ? bar1 : bar0, x0 / 2, y0, pnx);
-      if (ring) {
-        const long long oh = rb_off(g, hxg, hyg, pnx);
-#pragma unroll
-        for (int c = 0; c < 10; ++c) cp_async8(&halo[(sn * 10 + c) * NHALO + tid], in.c[c] + oh);
-      }
-    }
+    if (it + NS - 1 < nit) issue(it + NS - 1);  // its stage was last read in iteration it - 1
     asm volatile("cp.async.commit_group;\n" ::: "memory");
 
     const double *cr = core + st * 10 * CORE;
-    double *ph = phs + (it % 3) * 4 * PH;
+    double *ph = phs + (it & 1) * 4 * PH;
     // own site of plane p: half, core and padded phi' positions
     const int hp = (hw + y0 + ty + p) & 1;
     const int co = (hp * TY + ty) * HM + t;
@@ -187,7 +199,9 @@ __global__ void __launch_bounds__(NT, 2)
     }
 
     if (it >= 2) {
-      const double *pp = phs + ((it + 2) % 3) * 4 * PH;  // phi' of plane p-1 (written last iteration)
+      // phi' of plane p-1, written last iteration; the barrier at the top of
+      // this iteration also ends last iteration's reads of the buffer written now
+      const double *pp = phs + ((it + 1) & 1) * 4 * PH;
       const int kk = wrapn(p - 1, N);
       const int nh = ((hw + y0 + ty + kk) & 1) ^ 1;  // the neighbours' half
       const int rx = (nh * PR + ty + 1) * PM;

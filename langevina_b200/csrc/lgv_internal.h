@@ -114,9 +114,14 @@ cudaError_t launch_batch_em_adj(const RepDesc *d, const DiffDesc *dd, const int 
 cudaError_t launch_batch_diff_copy(const RepDesc *d, const DiffDesc *dd, const int *rep, const int *first,
                                    int nblocks, int dir, int phase, int s, int b, int S, cudaStream_t st);
 
+// planes per block of the batched heat-bath and charge kernels: their block
+// map holds nchunk * ceil(N / kBatchPlanes) blocks per replica
+constexpr int kBatchPlanes = 4;
+
 // phase_phi / phase_q: which buffer holds the current phi / charges
 cudaError_t launch_batch_ideal(const RepDesc *d, const int *rep, const int *first, int nblocks, int tile,
                                int phase_phi, int phase_q, double dt, cudaStream_t st);
+// rep / first / nblocks of launch_batch_hb and launch_batch_charge: the slab map (kBatchPlanes planes per block)
 cudaError_t launch_batch_hb(const RepDesc *d, const EnsDyn *dyn, const int *rep, const int *first, int nblocks,
                             int phase_phi, int parity, double dt, int ctr_off, cudaStream_t st);
 cudaError_t launch_batch_charge(const RepDesc *d, const EnsDyn *dyn, const int *rep, const int *first, int nblocks,

@@ -1512,22 +1512,36 @@ __device__ __forceinline__ bool plane_coords(const RepDesc &r, int local, int &m
   return j < r.g.N;
 }
 
+// slab kernels: a block covers 128 consecutive (j, m) elements of kBatchPlanes
+// consecutive planes of one replica, so the block-map and descriptor loads
+// (two dependent round trips before the first site load) are paid once per
+// kBatchPlanes planes
+__device__ __forceinline__ bool slab_coords(const RepDesc &r, int local, int &m, int &j, int &k0) {
+  const int chunk = local % r.nchunk;
+  k0 = (local / r.nchunk) * kBatchPlanes;
+  const int t = chunk * 128 + (int)threadIdx.x;
+  j = t / r.g.H;
+  m = t - j * r.g.H;
+  return j < r.g.N;
+}
+
 __global__ void __launch_bounds__(128) batch_hb_kernel(const RepDesc *__restrict__ d, const EnsDyn *__restrict__ dyn,
                                                        const int *__restrict__ rep, const int *__restrict__ first,
                                                        int phase, int parity, double dt, int ctr_off) {
   const int r = rep[blockIdx.x];
   const RepDesc &R = d[r];
   const EnsDyn y = *dyn;
-  int m, j, k;
-  if (!plane_coords(R, blockIdx.x - first[r], m, j, k)) return;
+  int m, j, k0;
+  if (!slab_coords(R, blockIdx.x - first[r], m, j, k0)) return;
   HbArgs a{};
   a.rdtg = sqrt(2. * dt * R.gamma);
   a.Lambda2 = 0.5 * (2. * 3. + rep_mass(R, y));
   a.lam4 = R.lambda / 4.;
   a.H = R.H;
   a.sk = sub_key(R.key, y.ctr + (unsigned long long)ctr_off);
+  const Fields f = rep_fields(R, phase, phase);
   MonLocal mon;
-  hb_site<false, false>(rep_fields(R, phase, phase), R.g, parity, a, m, j, k, mon);
+  for (int k = k0; k < min(k0 + kBatchPlanes, R.g.N); ++k) hb_site<false, false>(f, R.g, parity, a, m, j, k, mon);
 }
 
 __global__ void __launch_bounds__(128) batch_charge_kernel(const RepDesc *__restrict__ d,
@@ -1537,8 +1551,8 @@ __global__ void __launch_bounds__(128) batch_charge_kernel(const RepDesc *__rest
   const int r = rep[blockIdx.x];
   const RepDesc &R = d[r];
   const EnsDyn y = *dyn;
-  int m, j, k;
-  if (!plane_coords(R, blockIdx.x - first[r], m, j, k)) return;
+  int m, j, k0;
+  if (!slab_coords(R, blockIdx.x - first[r], m, j, k0)) return;
   // the replica's pass order (counter mode of ModelGChargeHB::step)
   const unsigned long long c0 = y.ctr + (unsigned long long)ctr_off_order;
   const uint64_t w = split_word(sub_key(R.key, c0), 0);
@@ -1556,8 +1570,10 @@ __global__ void __launch_bounds__(128) batch_charge_kernel(const RepDesc *__rest
   a.inv2chi = 1.0 / (2. * R.chi);
   a.sk = sub_key(R.key, c0 + 1 + pass);
   a.pass = pass;
+  const Fields f = rep_fields(R, phase, phase);
   MonLocal mon;
-  charge_link_site<false, false>(rep_fields(R, phase, phase), R.g, dir, eoA, a, m, j, k, mon);
+  for (int k = k0; k < min(k0 + kBatchPlanes, R.g.N); ++k)
+    charge_link_site<false, false>(f, R.g, dir, eoA, a, m, j, k, mon);
 }
 
 // ---- differentiable Euler-Maruyama runs of an ensemble ---------------------
