@@ -41,6 +41,7 @@ ALG_BYTES = {  # algorithmic bytes per site, per launch (each input read once, e
     "em": 64.0,
 }
 STEP_BYTES = {"PV2HBSplit23": 1440.0, "PV2HBSplit11": 800.0}
+NOMINAL_HBM_GBS = 7700.0  # B200 HBM3e, HGX figure
 KCLASS = {"ideal": 0, "phi_hb": 1, "charge": 2, "em": 3, "measure": 4}
 COEF = dict(mass0=-4.813, lam=10.0, H=0.003, chi=5.0, gamma=1.0, diffusion=1.0 / 3.0)
 DT = 0.04
@@ -60,6 +61,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-variants", action="store_true")
     return ap.parse_args()
 
 
@@ -520,7 +522,8 @@ def run_ours(a):
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
                 if peak_kind == "measured" else "fallback 6.65 TB/s",
-                "traffic": traffic, "alg_bytes_per_launch": alg, "avg_launch_ms": avg_ms}
+                "traffic": traffic, "alg_bytes_per_launch": alg, "avg_launch_ms": avg_ms,
+                "frac_of_nominal": achieved / NOMINAL_HBM_GBS, "nominal_GBps": NOMINAL_HBM_GBS}
     kernels = {k: {"launches": kern[k][1], "total_ms": kern[k][0],
                    "avg_ms": (kern[k][0] / kern[k][1]) if kern[k][1] else None,
                    "alg_GBps": (ALG_BYTES[k] * V / (kern[k][0] / kern[k][1] / 1e3) / 1e9)
@@ -563,6 +566,28 @@ def run_ours(a):
                "sample": f"{done} {name} steps on a {Ns}^3 sample lattice ({el:.1f} s), oracle port with the "
                          f"reference serial RNG, one thread per emulated MPI rank"}
 
+    # ---- the other steppers on the same 256^3 lattice ---------------------------
+    variants = None
+    if rank == 0 and world == 1 and not a.no_variants:
+        variants = {}
+        for vname, ev, inner, outer, dt, bytes_site in (
+                ("PV2HBSplit11", L.PV2HBSPLIT, 1, 1, DT, 800.0),
+                ("EulerLangevinHB (Model A heat-bath sweep)", L.EULER_LANGEVIN_HB, 1, 1, DT / 6, 64.0),
+                ("ModelAEulerMaruyama", L.MODELA_EM, 1, 1, 0.02, 64.0)):
+            nst = 20
+            L.check(lib.lgv_step(h, ev, inner, outer, dt, 0.0, 3), "variant warm-up")
+            torch.cuda.synchronize()
+            v0, v1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            v0.record(stream)
+            L.check(lib.lgv_step(h, ev, inner, outer, dt, 0.0, nst), "variant")
+            v1.record(stream)
+            torch.cuda.synchronize()
+            vms = v0.elapsed_time(v1) / nst
+            variants[vname] = {"ms_per_step": vms, "site_updates_per_s": V / (vms / 1e3),
+                               "alg_bytes_per_site": bytes_site,
+                               "hbm_frac": bytes_site * V / (vms / 1e3) / 1e9 / peak,
+                               "steps": nst, "dt": dt}
+
     lgv_destroy = lib.lgv_destroy
     lgv_destroy(h)
     ensemble = None
@@ -592,6 +617,7 @@ def run_ours(a):
         "e2e": e2e,
         "ensemble": ensemble,
         "adjoint": adjoint,
+        "variants": variants,
         "gpu_launches": launches,
         "clocks": ck,
     }
