@@ -157,6 +157,23 @@ __device__ __forceinline__ void quatmul(const double a[4], const double b[4], do
   w[3] = (a[1] * b[2] - b[1] * a[2]) + b[0] * a[3] + a[0] * b[3];
 }
 
+// Charge advection of the ideal step at one site (Stepper.cxx:99-166).  The
+// reference's forward and backward difference terms, summed over the three
+// directions with equal spacing, reduce to
+//   n_A,l += dt [a2 (c_0 S_l - c_l S_0) - H c_l]            l = 1..3
+//   n_V,s += dt a2 (c_s1 S_s2 - c_s2 S_s1)                 (s, s1, s2) cyclic
+// with c = phi' at the site and S the sum of phi' over its six neighbours.
+__device__ __forceinline__ void charge_currents(const double c[4], const double S[4], double dt, double a2,
+                                                double H, double q[6]) {
+#pragma unroll
+  for (int l = 0; l < 3; ++l) q[l] += dt * (a2 * (c[0] * S[l + 1] - c[l + 1] * S[0]) - H * c[l + 1]);
+#pragma unroll
+  for (int s = 0; s < 3; ++s) {
+    const int s1 = 1 + (s + 1) % 3, s2 = 1 + (s + 2) % 3;
+    q[3 + s] += dt * (a2 * (c[s1] * S[s2] - c[s2] * S[s1]));
+  }
+}
+
 // In-place O(4) rotation phi <- L phi R with R = exp(-(muV - muA)/2),
 // L = exp((muV + muA)/2) (O4Rotation, O4AlgebraHelper.h:78-97).
 __device__ __forceinline__ void o4_rotate(const double muV[3], const double muA[3], double phi[4]) {

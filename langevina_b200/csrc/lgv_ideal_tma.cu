@@ -216,23 +216,10 @@ __global__ void __launch_bounds__(NT, 2)
         ym[l] = pp[l * PH + oym];
       }
       const double *c = pc, *zp = pn, *zm = pm;
-      // axial charges (Stepper.cxx:112-133)
+      double S[4];
 #pragma unroll
-      for (int l = 0; l < 3; ++l) {
-        const double bx = -xp[0] * c[l + 1] + c[0] * xp[l + 1] + c[0] * xm[l + 1] - xm[0] * c[l + 1];
-        const double by = -yp[0] * c[l + 1] + c[0] * yp[l + 1] + c[0] * ym[l + 1] - ym[0] * c[l + 1];
-        const double bz = -zp[0] * c[l + 1] + c[0] * zp[l + 1] + c[0] * zm[l + 1] - zm[0] * c[l + 1];
-        qc[l] += a.dt * (bx * a.a2 + by * a.a2 + bz * a.a2 - a.H * c[l + 1]);
-      }
-      // vector charges, epsilon = +1 for the cyclic (s, s+1, s+2) (Stepper.cxx:135-163)
-#pragma unroll
-      for (int s = 0; s < 3; ++s) {
-        const int s1 = 1 + (s + 1) % 3, s2 = 1 + (s + 2) % 3;
-        const double bx = xp[s2] * c[s1] - c[s2] * xm[s1] - xp[s1] * c[s2] + c[s1] * xm[s2];
-        const double by = yp[s2] * c[s1] - c[s2] * ym[s1] - yp[s1] * c[s2] + c[s1] * ym[s2];
-        const double bz = zp[s2] * c[s1] - c[s2] * zm[s1] - zp[s1] * c[s2] + c[s1] * zm[s2];
-        qc[3 + s] += a.dt * (bx * a.a2 + by * a.a2 + bz * a.a2);
-      }
+      for (int l = 0; l < 4; ++l) S[l] = ((xp[l] + xm[l]) + (yp[l] + ym[l])) + (zp[l] + zm[l]);
+      charge_currents(c, S, a.dt, a.a2, a.H, qc);
       // second half rotation on a copy: pc (phi') stays the z-1 neighbour of the next plane
       double pf[4] = {pc[0], pc[1], pc[2], pc[3]};
       rotate_site(pf, qc, a.dto2chi);

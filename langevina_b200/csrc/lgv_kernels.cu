@@ -1125,23 +1125,10 @@ __device__ __forceinline__ void ideal_tile(const Fields &in, const Fields &out, 
         ym[l] = pp[l * SP + sc - SX];
       }
       const double *c = pc, *zp = pn, *zm = pm;
-      // axial charges (Stepper.cxx:112-133)
+      double S[4];
 #pragma unroll
-      for (int l = 0; l < 3; ++l) {
-        const double bx = -xp[0] * c[l + 1] + c[0] * xp[l + 1] + c[0] * xm[l + 1] - xm[0] * c[l + 1];
-        const double by = -yp[0] * c[l + 1] + c[0] * yp[l + 1] + c[0] * ym[l + 1] - ym[0] * c[l + 1];
-        const double bz = -zp[0] * c[l + 1] + c[0] * zp[l + 1] + c[0] * zm[l + 1] - zm[0] * c[l + 1];
-        qc[l] += a.dt * (bx * a.a2 + by * a.a2 + bz * a.a2 - a.H * c[l + 1]);
-      }
-      // vector charges, epsilon = +1 for the cyclic (s, s+1, s+2) (Stepper.cxx:135-163)
-#pragma unroll
-      for (int s = 0; s < 3; ++s) {
-        const int s1 = 1 + (s + 1) % 3, s2 = 1 + (s + 2) % 3;
-        const double bx = xp[s2] * c[s1] - c[s2] * xm[s1] - xp[s1] * c[s2] + c[s1] * xm[s2];
-        const double by = yp[s2] * c[s1] - c[s2] * ym[s1] - yp[s1] * c[s2] + c[s1] * ym[s2];
-        const double bz = zp[s2] * c[s1] - c[s2] * zm[s1] - zp[s1] * c[s2] + c[s1] * zm[s2];
-        qc[3 + s] += a.dt * (bx * a.a2 + by * a.a2 + bz * a.a2);
-      }
+      for (int l = 0; l < 4; ++l) S[l] = ((xp[l] + xm[l]) + (yp[l] + ym[l])) + (zp[l] + zm[l]);
+      charge_currents(c, S, a.dt, a.a2, a.H, qc);
       // second half rotation on a copy: pc (phi') stays the z-1 neighbour of the next plane
       double pf[4] = {pc[0], pc[1], pc[2], pc[3]};
       rotate_site(pf, qc, a.dto2chi);
@@ -1919,23 +1906,13 @@ __global__ void __launch_bounds__(128) ideal_adj_a_kernel(Fields u, Fields lin, 
         zp[l] = P[sn.o[4]];
         zm[l] = P[sn.o[5]];
       }
-      double q2[6];
-      // n' exactly as the forward computes it (ideal_tile)
+      // n' exactly as the forward computes it (ideal_tile, ideal_tma_kernel)
+      double q2[6], S[4];
 #pragma unroll
-      for (int l = 0; l < 3; ++l) {
-        const double bx = -xp[0] * c[l + 1] + c[0] * xp[l + 1] + c[0] * xm[l + 1] - xm[0] * c[l + 1];
-        const double by = -yp[0] * c[l + 1] + c[0] * yp[l + 1] + c[0] * ym[l + 1] - ym[0] * c[l + 1];
-        const double bz = -zp[0] * c[l + 1] + c[0] * zp[l + 1] + c[0] * zm[l + 1] - zm[0] * c[l + 1];
-        q2[l] = u.c[4 + l][sn.own] + a.dt * (bx * a.a2 + by * a.a2 + bz * a.a2 - a.H * c[l + 1]);
-      }
+      for (int l = 0; l < 4; ++l) S[l] = ((xp[l] + xm[l]) + (yp[l] + ym[l])) + (zp[l] + zm[l]);
 #pragma unroll
-      for (int s = 0; s < 3; ++s) {
-        const int s1 = 1 + (s + 1) % 3, s2 = 1 + (s + 2) % 3;
-        const double bx = xp[s2] * c[s1] - c[s2] * xm[s1] - xp[s1] * c[s2] + c[s1] * xm[s2];
-        const double by = yp[s2] * c[s1] - c[s2] * ym[s1] - yp[s1] * c[s2] + c[s1] * ym[s2];
-        const double bz = zp[s2] * c[s1] - c[s2] * zm[s1] - zp[s1] * c[s2] + c[s1] * zm[s2];
-        q2[3 + s] = u.c[7 + s][sn.own] + a.dt * (bx * a.a2 + by * a.a2 + bz * a.a2);
-      }
+      for (int s = 0; s < 6; ++s) q2[s] = u.c[4 + s][sn.own];
+      charge_currents(c, S, a.dt, a.a2, a.H, q2);
       double ob[4], pb[4], qb[6];
 #pragma unroll
       for (int l = 0; l < 4; ++l) ob[l] = lin.c[l][sn.own];
