@@ -2,18 +2,27 @@
 // measurer.  FP64 throughout; HBM-bound stencils, no tensor-core work.
 //
 // Kernel map (reference loop each one replaces):
-//   hb_sweep_kernel     EulerLangevinHB::step, both checkerboard parities in
-//                       one z-marching launch (Stepper.cxx:287-389)
+//   hb_pass_kernel      EulerLangevinHB::step, one checkerboard parity per
+//                       launch (Stepper.cxx:287-389)
+//   hb_sweep_kernel     the same, both parities in one z-marching launch (opt-in)
 //   charge_pass_kernel  ModelGChargeHB::step, one (direction, parity) face
 //                       (Stepper.cxx:471-518, modelg_update_charge_pair :419-441)
-//   charge_x_kernel,    both faces of one direction per launch (x: whole rows
-//   charge_line_kernel  per CTA; y, z: streamed lines with a two-site halo)
+//   charge_slab_kernel, both faces of one direction per launch (opt-in):
+//   charge_x_kernel,    shared-memory slabs for N divisible by 32, otherwise x
+//   charge_line_kernel  rows per CTA and y, z streamed lines with two-site halos
 //   ideal_kernel        IdealPV2::step_no_reject fused: half rotation, charge
-//                       advection stencil, half rotation (Stepper.cxx:68-202)
+//                       advection stencil, half rotation (Stepper.cxx:68-202);
+//                       the TMA-staged ideal_tma_kernel (lgv_ideal_tma.cu)
+//                       replaces it for N divisible by 32
 //   em_kernel           Euler-Maruyama Model A step (action of Stepper.cxx:354-355)
 //   energy_*            IdealPV2::computeEnergy (Stepper.cxx:204-268)
 //   meas_*              Measurer::computeSliceAverage / ...Phase /
 //                       computeDerivedObs (measurer.cxx:10-317)
+//   batch_*             the same steps for every replica of an ensemble in one
+//                       launch (no counterpart: the reference runs one lattice)
+//   em_adjoint_kernel, rot_phi_kernel, ideal_adj_a/b_kernel, batch_em_*
+//                       adjoints of the Euler-Maruyama and ideal steps for the
+//                       differentiable runs (no counterpart)
 #include "lgv_internal.h"
 
 #include <algorithm>
