@@ -86,11 +86,13 @@ __device__ __forceinline__ void grid_sum4(double (&v)[4], double *partial, unsig
 }
 
 // Flat site-pair index -> (m, j, k) of the red-black half rows: idx = (k N + j) H + m.
+// 32-bit unsigned divisions (64-bit ones are emulated); idx < V/2 <= 2^32 for N <= 2048.
 __device__ __forceinline__ void pair_coords(long long idx, const Geo &g, int &m, int &j, int &k) {
-  const long long row = idx / g.H;
-  m = (int)(idx - row * g.H);
-  k = (int)(row / g.N);
-  j = (int)(row - (long long)k * g.N);
+  const unsigned u = (unsigned)idx, H = (unsigned)g.H, N = (unsigned)g.N;
+  const unsigned row = u / H;
+  m = (int)(u - row * H);
+  k = (int)(row / N);
+  j = (int)(row - (unsigned)k * N);
 }
 
 // Per-thread monitor tally, reduced per block and added once per block.
@@ -341,12 +343,36 @@ __device__ __forceinline__ void hb_site(const Fields &f, const Geo &g, int parit
   if (a.flags) a.flags[nat] = d.flag;
 }
 
-// Grid: (m chunks, j, k), so no 64-bit index division.
-template <bool INJECTED, bool MON>
+// Site of this thread in a one-parity pass.  ROWS (half rows a multiple of
+// 128 long): grid (H/128, N, N), no index arithmetic.  Otherwise grid
+// (N*H/128 rounded up, N): the sites of plane k are flat over the x blocks,
+// so no lanes idle when a half row is shorter than the block (N < 256).
+template <bool ROWS>
+__device__ __forceinline__ bool pass_site(const Geo &g, int &m, int &j, int &k) {
+  if (ROWS) {
+    m = blockIdx.x * 128 + threadIdx.x;
+    j = blockIdx.y;
+    k = blockIdx.z;
+    return true;
+  }
+  const unsigned t = blockIdx.x * 128 + threadIdx.x, H = (unsigned)g.H;
+  if (t >= (unsigned)g.N * H) return false;
+  const unsigned jj = t / H;
+  m = (int)(t - jj * H);
+  j = (int)jj;
+  k = blockIdx.y;
+  return true;
+}
+
+__host__ __forceinline__ dim3 pass_grid(const Geo &g, bool rows) {
+  return rows ? dim3(g.H / 128, g.N, g.N) : dim3((unsigned)(((long long)g.N * g.H + 127) / 128), g.N);
+}
+
+template <bool INJECTED, bool MON, bool ROWS>
 __global__ void __launch_bounds__(128) hb_pass_kernel(Fields f, Geo g, int parity, HbArgs a) {
-  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  int m, j, k;
   MonLocal mon;
-  if (m < g.H) hb_site<INJECTED, MON>(f, g, parity, a, m, blockIdx.y, blockIdx.z, mon);
+  if (pass_site<ROWS>(g, m, j, k)) hb_site<INJECTED, MON>(f, g, parity, a, m, j, k, mon);
   if (MON) mon_flush(mon, a.mon);
 }
 
@@ -558,12 +584,12 @@ __device__ __forceinline__ void charge_link_site(const Fields &f, const Geo &g, 
   }
 }
 
-// Grid: (m chunks, j, k).
-template <bool INJECTED, bool MON>
+// Grid as hb_pass_kernel (pass_site).
+template <bool INJECTED, bool MON, bool ROWS>
 __global__ void __launch_bounds__(128) charge_pass_kernel(Fields f, Geo g, int dir, int eoA, ChargeArgs a) {
-  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  int m, j, k;
   MonLocal mon;
-  if (m < g.H) charge_link_site<INJECTED, MON>(f, g, dir, eoA, a, m, blockIdx.y, blockIdx.z, mon);
+  if (pass_site<ROWS>(g, m, j, k)) charge_link_site<INJECTED, MON>(f, g, dir, eoA, a, m, j, k, mon);
   if (MON) mon_flush(mon, a.mon);
 }
 
@@ -2058,15 +2084,15 @@ static cudaError_t allow_smem(K kernel, size_t bytes) {
 
 cudaError_t launch_hb_pass(Fields f, int N, int parity, const HbArgs &a, cudaStream_t st) {
   const Geo g = make_geo(N);
-  dim3 grid((g.H + 127) / 128, N, N);
+  const bool rows = g.H % 128 == 0;
+  const dim3 grid = pass_grid(g, rows);
   const bool inj = a.prop != nullptr, mon = a.mon != nullptr;
-  if (inj) {
-    if (mon) hb_pass_kernel<true, true><<<grid, 128, 0, st>>>(f, g, parity, a);
-    else hb_pass_kernel<true, false><<<grid, 128, 0, st>>>(f, g, parity, a);
-  } else {
-    if (mon) hb_pass_kernel<false, true><<<grid, 128, 0, st>>>(f, g, parity, a);
-    else hb_pass_kernel<false, false><<<grid, 128, 0, st>>>(f, g, parity, a);
-  }
+#define LGV_HBP(I, M)                                                                                        \
+  if (rows) hb_pass_kernel<I, M, true><<<grid, 128, 0, st>>>(f, g, parity, a);                              \
+  else hb_pass_kernel<I, M, false><<<grid, 128, 0, st>>>(f, g, parity, a)
+  if (inj) { if (mon) { LGV_HBP(true, true); } else { LGV_HBP(true, false); } }
+  else { if (mon) { LGV_HBP(false, true); } else { LGV_HBP(false, false); } }
+#undef LGV_HBP
   return cudaGetLastError();
 }
 
@@ -2108,16 +2134,15 @@ cudaError_t launch_hb_sweep(Fields in, Fields out, int N, const HbArgs &a, cudaS
 
 cudaError_t launch_charge_pass(Fields f, int N, int dir, int eoA, const ChargeArgs &a, cudaStream_t st) {
   const Geo g = make_geo(N);
-  dim3 grid((g.H + 127) / 128, N, N);
-  const bool inj = a.q != nullptr;
-  const bool mon = a.mon != nullptr;
-  if (inj) {
-    if (mon) charge_pass_kernel<true, true><<<grid, 128, 0, st>>>(f, g, dir, eoA, a);
-    else charge_pass_kernel<true, false><<<grid, 128, 0, st>>>(f, g, dir, eoA, a);
-  } else {
-    if (mon) charge_pass_kernel<false, true><<<grid, 128, 0, st>>>(f, g, dir, eoA, a);
-    else charge_pass_kernel<false, false><<<grid, 128, 0, st>>>(f, g, dir, eoA, a);
-  }
+  const bool rows = g.H % 128 == 0;
+  const dim3 grid = pass_grid(g, rows);
+  const bool inj = a.q != nullptr, mon = a.mon != nullptr;
+#define LGV_CHP(I, M)                                                                                        \
+  if (rows) charge_pass_kernel<I, M, true><<<grid, 128, 0, st>>>(f, g, dir, eoA, a);                        \
+  else charge_pass_kernel<I, M, false><<<grid, 128, 0, st>>>(f, g, dir, eoA, a)
+  if (inj) { if (mon) { LGV_CHP(true, true); } else { LGV_CHP(true, false); } }
+  else { if (mon) { LGV_CHP(false, true); } else { LGV_CHP(false, false); } }
+#undef LGV_CHP
   return cudaGetLastError();
 }
 
