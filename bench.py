@@ -225,12 +225,15 @@ def run_ensemble(steps=20, plain_steps=2):
         for h in hs:
             L.check(lib.lgv_step(h, L.PV2HBSPLIT, 2, 3, DT, 0.0, 1), "warm")
         torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        for _ in range(plain_steps):
-            for h in hs:
-                L.check(lib.lgv_step(h, L.PV2HBSPLIT, 2, 3, DT, 0.0, 1), "step")
-        torch.cuda.synchronize()
-        plain[mode] = (time.perf_counter() - t0) / plain_steps * 1e3
+        best = float("inf")
+        for _ in range(3):  # best of three rounds: the loop's host timing is noisy
+            t0 = time.perf_counter()
+            for _ in range(plain_steps):
+                for h in hs:
+                    L.check(lib.lgv_step(h, L.PV2HBSPLIT, 2, 3, DT, 0.0, 1), "step")
+            torch.cuda.synchronize()
+            best = min(best, (time.perf_counter() - t0) / plain_steps * 1e3)
+        plain[mode] = best
         for h in hs:
             lib.lgv_destroy(h)
     best_plain = min(plain.values())
@@ -245,7 +248,7 @@ def run_ensemble(steps=20, plain_steps=2):
         "plain_ms_per_step": plain, "plain_replica_steps_per_s": R / (best_plain / 1e3),
         "speedup_vs_plain": best_plain / ms,
         "timing": "batched: CUDA events over graph replays; plain: host wall clock around a loop of lgv_step, "
-                  "one replica per call (one shared stream / each handle on its own stream)",
+                  "one replica per call (one shared stream / each handle on its own stream), best of three rounds",
     }
 
 

@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <numeric>
@@ -65,7 +66,9 @@ struct lgv_ensemble {
   std::vector<double *> bufs;
   RepDesc *dd = nullptr;
   EnsDyn *dyn = nullptr;
-  BlockMap ideal_map, plane_map, slab_map;
+  BlockMap ideal_map, plane_map, slab_map, tma_map;  // tma_map: ideal step of the TMA replicas
+  std::vector<char> tma_ok;                          // replica r takes the TMA ideal kernel
+  void *gmaps = nullptr;                             // their tensor maps, [R][2][2][10] x 128 B
   double *partial = nullptr, *oavg = nullptr;
   cudaStream_t own = nullptr, stream = nullptr;
   int phase_phi = 0, phase_q = 0;
@@ -140,7 +143,7 @@ int build_map(lgv_ensemble *e, BlockMap &m, const std::vector<int> &blocks_per_r
     rep.insert(rep.end(), blocks_per_rep[r], r);
   }
   m.nblocks = (int)rep.size();
-  ECK(cudaMalloc((void **)&m.rep, rep.size() * sizeof(int)));
+  ECK(cudaMalloc((void **)&m.rep, std::max<size_t>(rep.size(), 1) * sizeof(int)));
   ECK(cudaMalloc((void **)&m.first, e->R * sizeof(int)));
   ECK(cudaMalloc((void **)&m.count, e->R * sizeof(int)));
   ECK(cudaMemcpy(m.rep, rep.data(), rep.size() * sizeof(int), cudaMemcpyHostToDevice));
@@ -149,12 +152,41 @@ int build_map(lgv_ensemble *e, BlockMap &m, const std::vector<int> &blocks_per_r
   return LGV_OK;
 }
 
+// Replicas with N divisible by 32 take the TMA ideal kernel: encode the
+// tensor maps of their component planes for every (phi buffer, charge
+// buffer) pairing once, since the buffers never move.  LGV_IDEAL_TMA=0 keeps
+// every replica on the cp.async kernel, as for single lattices.
+int tensor_maps(lgv_ensemble *e) {
+  const char *env = std::getenv("LGV_IDEAL_TMA");
+  const bool off = env && env[0] == '0';
+  e->tma_ok.assign(e->R, 0);
+  std::vector<unsigned char> host((size_t)e->R * 40 * 128, 0);
+  bool any = false;
+  for (int r = 0; r < e->R; ++r) {
+    const RepDesc &d = e->hd[r];
+    if (off || !lgv::ideal_tma_supported(d.g.N)) continue;
+    bool ok = true;
+    for (int pphi = 0; pphi < 2 && ok; ++pphi)
+      for (int pq = 0; pq < 2 && ok; ++pq)
+        for (int c = 0; c < 10 && ok; ++c) {
+          const double *plane = d.base[c < 4 ? pphi : pq] + (size_t)c * d.pstride;
+          ok = lgv::tma_plane_map(plane, d.g.N, &host[(((size_t)r * 2 + pphi) * 2 + pq) * 10 * 128 + (size_t)c * 128]);
+        }
+    e->tma_ok[r] = ok ? 1 : 0;
+    any = any || ok;
+  }
+  if (!any) return LGV_OK;
+  ECK(cudaMalloc(&e->gmaps, host.size()));
+  ECK(cudaMemcpy(e->gmaps, host.data(), host.size(), cudaMemcpyHostToDevice));
+  return LGV_OK;
+}
+
 // (Re)derive the per-replica launch geometry for the current tuning and
 // upload the descriptors and block maps.
 int configure(lgv_ensemble *e) {
   int tx = 32, ty = 8;
   lgv::ideal_tile_dims(e->tile, &tx, &ty);
-  std::vector<int> ib(e->R), pb(e->R), sb(e->R);
+  std::vector<int> ib(e->R), pb(e->R), sb(e->R), tb(e->R);
   for (int r = 0; r < e->R; ++r) {
     RepDesc &d = e->hd[r];
     const int N = d.g.N;
@@ -163,12 +195,14 @@ int configure(lgv_ensemble *e) {
     d.igy = (N + ty - 1) / ty;
     d.izc = std::min(e->zchunk, N);
     d.igz = (N + d.izc - 1) / d.izc;
-    ib[r] = d.igx * d.igy * d.igz;
+    ib[r] = e->tma_ok[r] ? 0 : d.igx * d.igy * d.igz;
+    tb[r] = e->tma_ok[r] ? lgv::batch_tma_blocks(N, d.izc) : 0;
     pb[r] = d.nchunk * N;
     sb[r] = d.nchunk * ((N + lgv::kBatchPlanes - 1) / lgv::kBatchPlanes);
   }
   ECK(cudaMemcpy(e->dd, e->hd.data(), e->R * sizeof(RepDesc), cudaMemcpyHostToDevice));
   ETRY(build_map(e, e->ideal_map, ib));
+  ETRY(build_map(e, e->tma_map, tb));
   ETRY(build_map(e, e->plane_map, pb));
   ETRY(build_map(e, e->slab_map, sb));
   if (e->partial) cudaFree(e->partial);
@@ -198,8 +232,12 @@ int enqueue_step(lgv_ensemble *e, int ev, int inner, int outer, double dt) {
   const int nb_i = e->ideal_map.nblocks, nb_p = e->plane_map.nblocks, nb_s = e->slab_map.nblocks;
   int off = 0;
   auto ideal = [&](double d) -> int {
-    ECK(lgv::launch_batch_ideal(e->dd, e->ideal_map.rep, e->ideal_map.first, nb_i, e->tile, e->phase_phi,
-                                e->phase_q, d, e->stream));
+    if (e->tma_map.nblocks > 0)
+      ECK(lgv::launch_batch_ideal_tma(e->dd, e->gmaps, e->tma_map.rep, e->tma_map.first, e->tma_map.nblocks,
+                                      e->phase_phi, e->phase_q, d, e->stream));
+    if (nb_i > 0)
+      ECK(lgv::launch_batch_ideal(e->dd, e->ideal_map.rep, e->ideal_map.first, nb_i, e->tile, e->phase_phi,
+                                  e->phase_q, d, e->stream));
     // the ideal step writes all ten components to the other buffer
     e->phase_phi ^= 1;
     e->phase_q ^= 1;
@@ -312,6 +350,7 @@ int lgv_ensemble_create(int nrep, const lgv_params *params, lgv_ensemble **out) 
       cudaMalloc((void **)&e->dyn, sizeof(EnsDyn)) != cudaSuccess ||
       cudaMalloc((void **)&e->oavg, (size_t)nrep * 11 * sizeof(double)) != cudaSuccess)
     return bail(efail(LGV_ERR_NOMEM, "ensemble tables"));
+  if ((rc = tensor_maps(e)) != LGV_OK) return bail(rc);
   if ((rc = configure(e)) != LGV_OK) return bail(rc);
   if (lgv::launch_ens_set(e->dyn, 0, 0.0, e->stream) != cudaSuccess || cudaStreamSynchronize(e->stream) != cudaSuccess)
     return bail(efail(LGV_ERR_CUDA, "ensemble init"));
@@ -327,6 +366,8 @@ int lgv_ensemble_destroy(lgv_ensemble *e) {
   free_map(e->ideal_map);
   free_map(e->plane_map);
   free_map(e->slab_map);
+  free_map(e->tma_map);
+  if (e->gmaps) cudaFree(e->gmaps);
   if (e->dd) cudaFree(e->dd);
   if (e->dyn) cudaFree(e->dyn);
   if (e->partial) cudaFree(e->partial);

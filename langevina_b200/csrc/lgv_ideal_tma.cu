@@ -11,8 +11,9 @@
 // half warp owns the sites of one x-parity, so every shared-memory access of
 // a half warp is 16 consecutive doubles.
 //
-// Used for N divisible by 32 (whole tiles; TMA strides need N/2 even); other
-// sizes and the batched ensembles use ideal_kernel.
+// Used for N divisible by 32 (whole tiles; TMA strides need N/2 even), for a
+// single lattice and for those replicas of an ensemble; other sizes use
+// ideal_kernel.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
@@ -86,7 +87,7 @@ __device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
 }
 
 // One thread: the 10 component boxes of plane k into core stage `dst`.
-__device__ __forceinline__ void issue_plane(const TmaMaps &maps, double *dst, unsigned bar, int m0, int j0, int k) {
+__device__ __forceinline__ void issue_plane(const CUtensorMap *maps, double *dst, unsigned bar, int m0, int j0, int k) {
   asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(kPlaneBytes) : "memory");
 #pragma unroll
@@ -94,13 +95,15 @@ __device__ __forceinline__ void issue_plane(const TmaMaps &maps, double *dst, un
     asm volatile(
         "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
         "[%6];\n" ::"r"(smem_addr(dst + c * CORE)),
-        "l"(&maps.m[c]), "r"(m0), "r"(j0), "r"(k), "r"(0), "r"(bar)
+        "l"(maps + c), "r"(m0), "r"(j0), "r"(k), "r"(0), "r"(bar)
         : "memory");
   }
 }
 
-__global__ void __launch_bounds__(NT, 2)
-    ideal_tma_kernel(const __grid_constant__ TmaMaps maps, Fields in, Fields out, Geo g, int zchunk, IdealArgs a) {
+// One CTA: tile (bx, by) of the xy plane, z-chunk bz.  maps: the tensor maps
+// of the 10 component planes of `in` (kernel parameters or global memory).
+__device__ __forceinline__ void ideal_tma_cta(const CUtensorMap *maps, const Fields &in, const Fields &out, const Geo &g,
+                                              int zchunk, const IdealArgs &a, int bx, int by, int bz) {
   extern __shared__ __align__(128) double smem_raw[];
   __shared__ __align__(8) unsigned long long mbar[NS];
   __shared__ int s_abort;
@@ -113,8 +116,8 @@ __global__ void __launch_bounds__(NT, 2)
   const int tid = threadIdx.x;
   const int ty = tid >> 5, hw = (tid >> 4) & 1, t = tid & 15;
   const int lx = 2 * t + hw;  // each half warp owns one x-parity of the row
-  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
-  const int z0 = blockIdx.z * zchunk;
+  const int x0 = bx * TX, y0 = by * TY;
+  const int z0 = bz * zchunk;
   const int z1 = min(z0 + zchunk, N);
   const int nit = (z1 - z0) + 2;
   const int xi = x0 + lx, yj = y0 + ty;
@@ -245,6 +248,44 @@ __global__ void __launch_bounds__(NT, 2)
   }
 }
 
+__global__ void __launch_bounds__(NT, 2)
+    ideal_tma_kernel(const __grid_constant__ TmaMaps maps, Fields in, Fields out, Geo g, int zchunk, IdealArgs a) {
+  ideal_tma_cta(maps.m, in, out, g, zchunk, a, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// Ensembles: the CTAs of every replica with N divisible by 32 in one launch,
+// through the same CTA body.  Replica r's maps for phi buffer pphi and charge
+// buffer pq are gmaps[((r * 2 + pphi) * 2 + pq) * 10 + c]; the host wrote them
+// before any launch, and the acquire fence orders those writes before the
+// tensor-map proxy reads them.
+__global__ void __launch_bounds__(NT, 2)
+    batch_ideal_tma_kernel(const RepDesc *__restrict__ d, const CUtensorMap *__restrict__ gmaps,
+                           const int *__restrict__ rep, const int *__restrict__ first, int pphi, int pq, double dt) {
+  const int r = rep[blockIdx.x];
+  const RepDesc &R = d[r];
+  const int l = blockIdx.x - first[r];
+  const int ntx = R.g.N / TX, nty = R.g.N / TY;
+  const int bx = l % ntx, by = (l / ntx) % nty, bz = l / (ntx * nty);
+  const CUtensorMap *maps = gmaps + ((size_t)(r * 2 + pphi) * 2 + pq) * 10;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int c = 0; c < 10; ++c)
+      asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;\n" ::"l"(maps + c) : "memory");
+  }
+  Fields in, out;
+#pragma unroll
+  for (int L = 0; L < 10; ++L) {
+    in.c[L] = R.base[L < 4 ? pphi : pq] + (long long)L * R.pstride;
+    out.c[L] = R.base[L < 4 ? (pphi ^ 1) : (pq ^ 1)] + (long long)L * R.pstride;
+  }
+  IdealArgs a;
+  a.dto2chi = (dt / 2.0) / R.chi;
+  a.dt = dt;
+  a.a2 = R.a2;
+  a.H = R.H;
+  ideal_tma_cta(maps, in, out, R.g, R.izc, a, bx, by, bz);
+}
+
 // ---------------------------------------------------------------------------
 // Tensor maps: one per component plane, 4-D view (m, j, k, half) of the
 // red-black layout; cached by (plane address, N).
@@ -306,6 +347,23 @@ cudaError_t launch_ideal_tma(Fields in, Fields out, int N, int zchunk, const Ide
   const Geo g = make_geo(N);
   dim3 grid(N / TX, N / TY, (unsigned)((N + zchunk - 1) / zchunk));
   ideal_tma_kernel<<<grid, NT, kSmemBytes, st>>>(maps, in, out, g, zchunk, a);
+  return cudaGetLastError();
+}
+
+int batch_tma_blocks(int N, int zchunk) { return (N / TX) * (N / TY) * ((N + zchunk - 1) / zchunk); }
+
+bool tma_plane_map(const double *plane, int N, void *out128) {
+  if (((uintptr_t)plane & 15) != 0) return false;
+  return plane_map(plane, N, reinterpret_cast<CUtensorMap *>(out128));
+}
+
+cudaError_t launch_batch_ideal_tma(const RepDesc *d, const void *gmaps, const int *rep, const int *first, int nblocks,
+                                   int phase_phi, int phase_q, double dt, cudaStream_t st) {
+  cudaError_t e = cudaFuncSetAttribute(batch_ideal_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)kSmemBytes);
+  if (e != cudaSuccess) return e;
+  batch_ideal_tma_kernel<<<nblocks, NT, kSmemBytes, st>>>(d, reinterpret_cast<const CUtensorMap *>(gmaps), rep, first,
+                                                          phase_phi, phase_q, dt);
   return cudaGetLastError();
 }
 

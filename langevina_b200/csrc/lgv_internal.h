@@ -203,6 +203,14 @@ cudaError_t launch_ideal(Fields in, Fields out, int N, const IdealArgs &a, cudaS
 // TMA-staged ideal step (lgv_ideal_tma.cu): N divisible by 32
 bool ideal_tma_supported(int N);
 cudaError_t launch_ideal_tma(Fields in, Fields out, int N, int zchunk, const IdealArgs &a, cudaStream_t st);
+// Ensembles: the TMA ideal step for replicas with N divisible by 32.
+// tma_plane_map encodes the 128-byte tensor map of one component plane; gmaps
+// holds, per replica r, buffer phases (pphi, pq) and component c, the map at
+// ((r * 2 + pphi) * 2 + pq) * 10 + c; a replica takes batch_tma_blocks(N, izc) blocks.
+bool tma_plane_map(const double *plane, int N, void *out128);
+int batch_tma_blocks(int N, int zchunk);
+cudaError_t launch_batch_ideal_tma(const RepDesc *d, const void *gmaps, const int *rep, const int *first, int nblocks,
+                                   int phase_phi, int phase_q, double dt, cudaStream_t st);
 // bounded device waits that gave up since the last clear
 unsigned read_wait_timeouts(bool clear);
 // energy: writes E into dev_out[0]; scratch >= energy_scratch_doubles(N)

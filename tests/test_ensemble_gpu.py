@@ -3,7 +3,8 @@ evolves like a lattice of its own (an lgv handle with the same params and
 counter), for every packing order, ideal tile shape and z-chunk, with and
 without CUDA-graph replay -- bit for bit through heat-bath, charge and
 Euler-Maruyama steps, and to 1-2 ulp through the ideal step (the same device
-code compiled into a second kernel); volume averages match the single-lattice
+code compiled into a second kernel; replicas with N divisible by 32 go
+through the TMA kernel's CTA body, the others through the cp.async one); volume averages match the single-lattice
 measurer; the autotuner restores state and counter."""
 import ctypes as C
 
@@ -29,7 +30,9 @@ def make(lgv, specs):
     return L, lib, e
 
 
-SPECS = [(8, 11, 0.003), (6, 12, 0.006), (16, 13, 0.012), (8, 14, 0.003), (34, 15, 0.006), (4, 16, 0.012)]
+# 32 takes the TMA ideal kernel, the other sizes the cp.async one, in the same step
+SPECS = [(8, 11, 0.003), (6, 12, 0.006), (16, 13, 0.012), (8, 14, 0.003), (34, 15, 0.006), (4, 16, 0.012),
+         (32, 17, 0.003)]
 
 
 def singles(lgv, specs, states, plan):
