@@ -486,10 +486,16 @@ int lgv_ensemble_step(lgv_ensemble *e, int evolver, int inner, int outer, double
       const int pp = e->phase_phi, pq = e->phase_q;
       const unsigned long long c0 = e->ctr;
       cudaGraph_t g = nullptr;
-      ECK(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+      // Capture on the ensemble's own stream: the caller's stream may be the
+      // legacy default stream, which cannot be captured.  The graph is then
+      // launched on the caller's stream.
+      cudaStream_t user = e->stream;
+      ECK(cudaStreamBeginCapture(e->own, cudaStreamCaptureModeThreadLocal));
+      e->stream = e->own;
       int rc = enqueue_step(e, evolver, inner, outer, dt);
       if (rc == LGV_OK) rc = enqueue_step(e, evolver, inner, outer, dt);
-      cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
+      cudaError_t ce = cudaStreamEndCapture(e->own, &g);
+      e->stream = user;
       e->phase_phi = pp;  // capture issued nothing: restore the host mirrors
       e->phase_q = pq;
       e->ctr = c0;

@@ -129,3 +129,33 @@ def test_noisy_substeps_are_bit_exact(lgv, ev, dt):
             assert np.array_equal(got, w)
     finally:
         lib.lgv_ensemble_destroy(e)
+
+
+def test_graphs_replay_on_the_legacy_default_stream(lgv):
+    """A caller's stream that cannot be captured (the legacy default stream,
+    passed as NULL) still gets graph replay: the ensemble captures on its own
+    stream and launches the graph on the caller's."""
+    specs = SPECS[:4]
+    states = [rand_state(N, 400 + i) for i, (N, _, _) in enumerate(specs)]
+    got = []
+    for stream in (None, 0):
+        L, lib, e = make(lgv, specs)
+        try:
+            L.check(lib.lgv_ensemble_use_graphs(e, 1), "graphs")
+            if stream is not None:
+                L.check(lib.lgv_ensemble_set_stream(e, C.c_void_p(stream)), "set_stream")
+            for r, u in enumerate(states):
+                L.check(lib.lgv_ensemble_set_state(e, r, L.ptr(u)), "set_state")
+            L.check(lib.lgv_ensemble_step(e, PV2, 2, 3, 0.04, 0.0, 4), "step")
+            L.check(lib.lgv_ensemble_step(e, HB, 1, 1, 0.02, 0.0, 3), "step")
+            L.check(lib.lgv_ensemble_synchronize(e), "sync")
+            out = []
+            for r, u in enumerate(states):
+                g = np.empty_like(u)
+                L.check(lib.lgv_ensemble_get_state(e, r, L.ptr(g)), "get_state")
+                out.append(g)
+            got.append(out)
+        finally:
+            lib.lgv_ensemble_destroy(e)
+    for a, b in zip(*got):
+        assert np.array_equal(a, b)

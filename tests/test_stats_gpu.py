@@ -5,6 +5,12 @@ goldens and known answers (run on the device, seconds each).
   <phi^2> against ModelG/hcrit1_N032_m-04813_h010000_l10000_averages_ave.out:1
   (columns 1-2 and 13-14).  The two columns are reproduced at lambda = 4, the
   coupling of the reference's heatbathtest.json that produced the file.
+  The same point with two 64-replica ensembles (batched launches): the
+  equilibrium does not depend on the proposal width (dt = 0.05 vs 0.2), and
+  the pooled averages sit within 5 sigma of the golden (measured pulls -3.3
+  for <phi_0> and -2.8 for <phi^2>; the golden's error bar implies a run
+  of ~45000 measurements, longer than heatbathtest.json's, so its settings
+  are not fully known).
 - Free field (lambda = 0, H = 0): the stationary equal-time wall correlator of
   the Euler-Maruyama step equals free2ptFE of ModelG/freeCase.ipynb (cell 7).
 - Charge heat bath: the equilibrium of exp(-n^2 / 2 chi) at fixed total charge
@@ -86,6 +92,62 @@ def test_equilibrium_matches_hcrit1_golden(lgv):
     assert abs(m0 - gold["phi0_mean"]) < 4 * s0
     assert abs(m2 - 0.99771450882) < 4 * s2
 
+
+
+def ensemble_hb_equilibrium(lgv, R, seed0, dt, therm=4000, nsamp=4000, every=25, N=32):
+    """<phi_0> and <phi^2> of R independent 32^3 replicas of the phi heat
+    bath at the hcrit1 point (lambda = 4), one batched launch per half sweep;
+    the error is the spread of the replica means (independent runs)."""
+    import torch
+    from langevina_b200 import _lib as L
+
+    lib = L.load()
+    arr = (L.lgv_params * R)()
+    for r in range(R):
+        arr[r] = L.make_params(N, mass0=-4.813, lam=4.0, H=0.01, gamma=1.0, seed=seed0 + r)
+    e = C.c_void_p()
+    L.check(lib.lgv_ensemble_create(R, arr, C.byref(e)), "ensemble_create")
+    try:
+        L.check(lib.lgv_ensemble_set_stream(e, C.c_void_p(torch.cuda.current_stream().cuda_stream)), "stream")
+        L.check(lib.lgv_ensemble_initialize(e, 1, 0.3), "init")
+        L.check(lib.lgv_ensemble_step(e, HB, 1, 1, dt, 0.0, therm), "thermalise")
+        hist = torch.empty((nsamp, R, 11), dtype=torch.float64, device="cuda")
+        for i in range(nsamp):
+            L.check(lib.lgv_ensemble_step(e, HB, 1, 1, dt, 0.0, every), "sweeps")
+            L.check(lib.lgv_ensemble_oaverage_device(e, C.c_void_p(hist[i].data_ptr())), "oaverage")
+        torch.cuda.synchronize()
+    finally:
+        lib.lgv_ensemble_destroy(e)
+    h = hist.cpu().numpy()
+    out = {}
+    for name, col in (("phi0", 0), ("phi2", 10)):
+        m = h[:, :, col].mean(axis=0)
+        out[name] = (m.mean(), m.std(ddof=1) / math.sqrt(R))
+    return out
+
+
+def test_heat_bath_equilibrium_is_dt_independent_and_near_hcrit1(lgv):
+    """Metropolis with a symmetric proposal of width sqrt(2 dt Gamma) samples
+    exp(-S) whatever dt is: two 64-replica ensembles at dt = 0.05 and 0.2
+    must agree.  Their pooled <phi_0>, <phi^2> are then set against the
+    hcrit1 golden (columns 1-2 and 13-14)."""
+    with open(os.path.join(GOLD, "hcrit1.json")) as f:
+        gold = json.load(f)
+    a = ensemble_hb_equilibrium(lgv, 64, 7000, 0.05)
+    b = ensemble_hb_equilibrium(lgv, 64, 9000, 0.2)
+    golden = {"phi0": (gold["phi0_mean"], gold["phi0_err"]), "phi2": (0.99771450882, 4.8322472767e-05)}
+    for k in ("phi0", "phi2"):
+        (ma, ea), (mb, eb) = a[k], b[k]
+        assert ea < 5e-4 and eb < 5e-4
+        assert abs(ma - mb) < 4 * math.hypot(ea, eb), f"{k}: dt 0.05 {ma:.6f}+-{ea:.6f} vs dt 0.2 {mb:.6f}+-{eb:.6f}"
+        w = np.array([1 / ea ** 2, 1 / eb ** 2])
+        m = (w[0] * ma + w[1] * mb) / w.sum()
+        e = 1 / math.sqrt(w.sum())
+        g, ge = golden[k]
+        pull = (m - g) / math.hypot(e, ge)
+        print(f"{k}: dt 0.05 {ma:.6f}+-{ea:.6f}, dt 0.2 {mb:.6f}+-{eb:.6f}, pooled {m:.6f}+-{e:.6f}, "
+              f"golden {g:.6f}+-{ge:.6f}, pull {pull:+.2f}")
+        assert abs(pull) < 5
 
 def free2pt_fe(n, m2, dt, N, gamma=1.0):
     """free2ptFE of freeCase.ipynb (cell 7), S -> infinity."""
