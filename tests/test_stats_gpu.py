@@ -93,7 +93,6 @@ def test_equilibrium_matches_hcrit1_golden(lgv):
     assert abs(m2 - 0.99771450882) < 4 * s2
 
 
-
 def ensemble_hb_equilibrium(lgv, R, seed0, dt, therm=4000, nsamp=4000, every=25, N=32):
     """<phi_0> and <phi^2> of R independent 32^3 replicas of the phi heat
     bath at the hcrit1 point (lambda = 4), one batched launch per half sweep;
@@ -148,6 +147,7 @@ def test_heat_bath_equilibrium_is_dt_independent_and_near_hcrit1(lgv):
         print(f"{k}: dt 0.05 {ma:.6f}+-{ea:.6f}, dt 0.2 {mb:.6f}+-{eb:.6f}, pooled {m:.6f}+-{e:.6f}, "
               f"golden {g:.6f}+-{ge:.6f}, pull {pull:+.2f}")
         assert abs(pull) < 5
+
 
 def free2pt_fe(n, m2, dt, N, gamma=1.0):
     """free2ptFE of freeCase.ipynb (cell 7), S -> infinity."""
