@@ -62,6 +62,7 @@ def parse():
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-variants", action="store_true")
+    ap.add_argument("--no-postprocess", action="store_true")
     return ap.parse_args()
 
 
@@ -473,6 +474,78 @@ def run_adjoint_batch(reps=3):
     }
 
 
+NOMINAL_FP64_TFLOPS = 37.0  # B200 dense FP64 (HGX B200 datasheet); no measured FP64 peak on this pool
+POST = dict(T=4096, N=256, ntmax=512, cpu_series=64)
+
+
+def run_postprocess(reps=5):
+    """Post-processing of a 256^3 run's measurement history on the device: the
+    k walls of the 11 observables on the 3 axes (3 x 11 x 129 complex series)
+    over T = 4096 measurements, their time correlators <O(t) O*(t + tau)>,
+    tau < 512 (computeOtOtp, Loader.py:229-254), and the x2k transform of the
+    T x 3 x 11 walls of 256 sites (x2k.cxx:94-113).  CUDA events, best of
+    `reps`; the CPU leg runs the numpy restatement of the same correlator on
+    64 of the series and scales by the series count."""
+    import torch
+
+    from langevina_b200 import postprocess as G
+
+    T, N, ntmax = POST["T"], POST["N"], POST["ntmax"]
+    NK = N // 2 + 1
+    ns = 3 * 11 * NK
+    gen = torch.Generator(device="cuda").manual_seed(11)
+    d = torch.randn((T, 3, 11, NK), dtype=torch.complex128, device="cuda", generator=gen)
+    dc = torch.conj(d).resolve_conj()
+    walls = torch.randn((T, 3, 11, N), dtype=torch.float64, device="cuda", generator=gen)
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        st = torch.cuda.current_stream()
+        torch.cuda.synchronize()
+        e0.record(st)
+        fn()
+        e1.record(st)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    corr = lambda: G.computeOtOtp(d, dc, nTMax=ntmax)  # noqa: E731
+    xk = lambda: G.x2k(walls)  # noqa: E731
+    corr(), xk()
+    tc = min(timed(corr) for _ in range(reps))
+    tx = min(timed(xk) for _ in range(reps))
+    macs = ns * sum(T - tau for tau in range(ntmax))
+    flops_c = 8.0 * macs
+    flops_x = 4.0 * (T * 3 * 11) * NK * N
+    out = {
+        "workload": f"measurement history of a {N}^3 run: T={T} samples of the k walls of 11 observables x 3 axes "
+                    f"({ns} complex series), correlators for tau < {ntmax}; x2k of T x 3 x 11 walls of {N} sites",
+        "correlator_ms": tc, "correlator_fp64_tflops": flops_c / (tc / 1e3) / 1e12,
+        "correlator_frac_of_nominal_fp64": flops_c / (tc / 1e3) / 1e12 / NOMINAL_FP64_TFLOPS,
+        "x2k_ms": tx, "x2k_fp64_tflops": flops_x / (tx / 1e3) / 1e12,
+        "nominal_fp64_tflops": NOMINAL_FP64_TFLOPS,
+        "flop_count": "8 per complex multiply-add of the correlator; 4 per real x complex twiddle term of x2k",
+        "timing": f"CUDA events, best of {reps}",
+    }
+    try:
+        sys.path.insert(0, os.path.join(REPO, "oracle"))
+        import postprocess as P  # the numpy restatement (CPU leg only)
+
+        k = POST["cpu_series"]
+        a = d.reshape(T, -1)[:, :k].cpu().numpy()
+        b = dc.reshape(T, -1)[:, :k].cpu().numpy()
+        t0 = time.perf_counter()
+        P.computeOtOtp(a, b, nTMax=ntmax)
+        el = time.perf_counter() - t0
+        cpu_ms = el * 1e3 * ns / k
+        out["cpu_baseline"] = {"correlator_ms": cpu_ms, "kind": "port", "cores": 1,
+                               "sample": f"numpy restatement of computeOtOtp on {k} of the {ns} series "
+                                         f"({el:.2f} s), scaled by the series count"}
+        out["speedup_vs_cpu"] = cpu_ms / tc
+    except Exception as exc:  # the CPU leg is a reported baseline only
+        out["cpu_baseline"] = {"unavailable": str(exc)}
+    return out
+
+
 def rank_env():
     """(world, rank, local rank) from the torchrun environment (1, 0, 0 without it)."""
     return (int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")),
@@ -666,6 +739,9 @@ def run_ours(a):
     config2 = None
     if world == 1 and not a.no_variants:
         config2 = run_config2()
+    postprocess = None
+    if world == 1 and not a.no_postprocess:
+        postprocess = run_postprocess()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -688,6 +764,7 @@ def run_ours(a):
         "adjoint": adjoint,
         "variants": variants,
         "config2": config2,
+        "postprocess": postprocess,
         "gpu_launches": launches,
         "clocks": ck,
     }

@@ -316,6 +316,35 @@ int lgv_ensemble_synchronize(lgv_ensemble *e);
 #define LGV_NOALLOC_MAX_N 128
 int lgv_measure_aos_noalloc(const double *dev_aos, int N, double *dev_out, void *stream);
 
+/* Post-processing of measurement histories held in device memory.  Stateless,
+ * asynchronous on `stream` (NULL = legacy default stream), no allocation,
+ * deterministic (every sum in a fixed order).
+ *
+ * lgv_x2k replaces the x2k.exe transform (ModelG/x2k.cxx:94-113): for every row
+ * of walls ([rows][N], N even, <= 8192), out[row][k] = (1/N) sum_x walls[row][x]
+ * e^{-2 pi i k x / N} for k = 0..N/2, stored as (re, im) pairs: out is
+ * [rows][N/2+1][2].  On a wall of lgv_measure it reproduces the measurer's k
+ * wall bit for bit. */
+int lgv_x2k(const double *walls, int64_t rows, int N, double *out, void *stream);
+/* lgv_x2k_rotated replaces x2k_rotated.exe (ModelG/x2k_rotated.cxx:92-143):
+ * walls_k is [rows][nfields >= 10][NK][2] (fields phi_0..3, A_1..3, V_1..3, ...
+ * as lgv_x2k writes them); per row the direction n is the real part of the four
+ * phi modes at k = 0, normalised ((1,0,0,0) below DBL_MIN), and out is
+ * [rows][13][NK][2]: phi along n, phi minus that (4), contract_rho(n, rho) (4),
+ * contract_rho(n, dual rho) (4). */
+int lgv_x2k_rotated(const double *walls_k, int64_t rows, int nfields, int NK, double *out, void *stream);
+/* lgv_time_correlator replaces computeOtOtp with its default mean statistic
+ * (python/Loader.py:229-254) for many series at once.  a and b are time-major:
+ * element t of series s is a[t*ld + s] (real) or the pair a[t*ld + 2s], +1
+ * (is_complex); T samples, nseries series, ld >= nseries (x2 if complex).  For
+ * tau = 0..ntmax-1: out[tau][s] = mean over t = 0, decim, 2 decim, ... < T - tau
+ * of a_s(t) * b_s(t + tau) (complex product, no conjugation), minus
+ * mean(a_s) * mean(b_s) over all T samples when conn != 0.  out is
+ * [ntmax][nseries] (x2 if complex).  1 <= ntmax <= T (the reference's slices
+ * past T - 1 are empty or wrap; they are rejected here). */
+int lgv_time_correlator(const double *a, const double *b, int64_t T, int64_t nseries, int64_t ld, int is_complex,
+                        int ntmax, int decim, int conn, double *out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -12,6 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liblgv.so")
 
 LGV_OK = 0
+LGV_ERR_INVALID, LGV_ERR_CUDA, LGV_ERR_NOMEM, LGV_ERR_TIMEOUT, LGV_ERR_STATE, LGV_ERR_UNSUPPORTED = -1, -2, -3, -4, -5, -6
 NPHI, NA, NV, NDOF = 4, 3, 3, 10
 NOBS, NOBS_PHASE = 11, 14
 NOALLOC_MAX_N = 128
@@ -104,6 +105,10 @@ SIGNATURES = [
     ("lgv_ensemble_diff_backward", C.c_int, [_H, C.c_void_p, C.c_void_p]),
     ("lgv_ensemble_set_stream", C.c_int, [_H, C.c_void_p]),
     ("lgv_ensemble_synchronize", C.c_int, [_H]),
+    ("lgv_x2k", C.c_int, [C.c_void_p, C.c_int64, C.c_int, C.c_void_p, C.c_void_p]),
+    ("lgv_x2k_rotated", C.c_int, [C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
+    ("lgv_time_correlator", C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_int, C.c_int,
+                                      C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
 ]
 
 _lib = None

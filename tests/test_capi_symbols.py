@@ -71,3 +71,20 @@ def test_create_rejects_bad_coefficients():
         setattr(p, field, bad)
         h = C.c_void_p()
         assert lib.lgv_create(C.byref(p), C.byref(h)) == -1
+
+
+def test_postprocess_argument_checks_need_no_gpu():
+    """Argument validation of the post-processing entry points runs before any
+    CUDA call (the dummy pointers are never dereferenced)."""
+    from langevina_b200 import _lib
+
+    lib = _lib.load()
+    d = C.c_void_p(16)
+    inv = _lib.LGV_ERR_INVALID
+    assert lib.lgv_x2k(None, 1, 8, d, None) == inv
+    assert lib.lgv_x2k(d, 1, 7, d, None) == inv  # odd N
+    assert lib.lgv_x2k(d, 0, 8, d, None) == _lib.LGV_OK  # nothing to do
+    assert lib.lgv_x2k_rotated(d, 1, 9, 5, d, None) == inv  # fewer than 10 fields
+    assert lib.lgv_time_correlator(d, d, 10, 2, 2, 0, 11, 1, 0, d, None) == inv  # ntmax > T
+    assert lib.lgv_time_correlator(d, d, 10, 2, 3, 1, 5, 1, 0, d, None) == inv  # ld below 2 * nseries
+    assert lib.lgv_time_correlator(d, d, 10, 2, 2, 0, 5, 0, 0, d, None) == inv  # decim 0
