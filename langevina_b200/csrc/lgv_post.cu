@@ -87,18 +87,31 @@ __global__ void __launch_bounds__(256) x2k_tile_kernel(const double *__restrict_
   if (lane >= nr) return;
   const double *row = tile + lane * S;
   double *o = out + (r0 + lane) * NK * 2;
-  for (int k = warp; k < NK; k += 8) {
-    double re = 0, im = 0;
-    int m = 0;
+  // four k per pass over the row (k, k + 8, k + 16, k + 24): each row value
+  // read from shared memory serves eight multiply-adds
+  for (int k0 = warp; k0 < NK; k0 += 32) {
+    double re[4] = {0, 0, 0, 0}, im[4] = {0, 0, 0, 0};
+    int m[4] = {0, 0, 0, 0}, dk[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) dk[q] = (k0 + 8 * q) % N;  // k itself for every k < NK; keeps m < N beyond
     for (int x = 0; x < N; ++x) {
       const double v = row[x];
-      re += v * tw[N + m];
-      im -= v * tw[m];
-      m += k;
-      if (m >= N) m -= N;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        re[q] += v * tw[N + m[q]];
+        im[q] -= v * tw[m[q]];
+        m[q] += dk[q];
+        if (m[q] >= N) m[q] -= N;
+      }
     }
-    o[k * 2] = re / (double)N;
-    o[k * 2 + 1] = im / (double)N;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int k = k0 + 8 * q;
+      if (k < NK) {
+        o[k * 2] = re[q] / (double)N;
+        o[k * 2 + 1] = im[q] / (double)N;
+      }
+    }
   }
 }
 
@@ -337,10 +350,10 @@ int lgv_time_correlator(const double *a, const double *b, int64_t T, int64_t nse
   if (ntmax < 1 || ntmax > T) return fail(LGV_ERR_INVALID, "lgv_time_correlator: 1 <= ntmax <= T");
   if (ld < nseries * (is_complex ? 2 : 1)) return fail(LGV_ERR_INVALID, "lgv_time_correlator: ld below the row width");
   const int G = is_complex ? kGCplx : kGReal;
-  const long long gx = (nseries + 31) / 32;
-  const long long gy = ((long long)ntmax + G * kCorrLagWarps - 1) / (G * kCorrLagWarps);
-  if (gx > 0x7fffffffLL || gy > 65535) return fail(LGV_ERR_INVALID, "lgv_time_correlator: grid too large");
-  const dim3 grid((unsigned)gx, (unsigned)gy), block(32, kCorrLagWarps);
+  const long long gs = (nseries + 31) / 32;
+  const long long gl = ((long long)ntmax + G * kCorrLagWarps - 1) / (G * kCorrLagWarps);
+  if (gs > 0x7fffffffLL || gl > 65535) return fail(LGV_ERR_INVALID, "lgv_time_correlator: grid too large");
+  const dim3 grid((unsigned)gs, (unsigned)gl), block(32, kCorrLagWarps);
   const bool vec = ((uintptr_t)a % 16 == 0) && ((uintptr_t)b % 16 == 0) && ld % 2 == 0;
   cudaStream_t st = (cudaStream_t)stream;
   if (is_complex && vec)
