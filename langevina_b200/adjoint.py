@@ -37,6 +37,9 @@ def _apply_theta(model, theta):
 def _snapshot(model):
     """Device copy of the lattice (AoS) and the noise counter."""
     buf = torch.empty(model.V * L.NDOF, dtype=torch.float64, device="cuda")
+    # the handle writes on its own stream: torch's pending work on memory its
+    # allocator may have handed out again must finish first
+    torch.cuda.current_stream().synchronize()
     L.check(model.lib.lgv_get_state_device(model.handle, C.c_void_p(buf.data_ptr())), "lgv_get_state_device")
     model.synchronize()
     return buf, model.get_counter()
