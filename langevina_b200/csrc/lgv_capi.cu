@@ -101,7 +101,11 @@ struct lgv_handle {
   // live per-kernel timing (lgv_timing_enable): event pairs around launches
   bool timing_on = false;
   std::vector<cudaEvent_t> ev_pool;
-  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_used;
+  struct TimedLaunch {
+    int cls, units;  // units: faces / passes the launch covers
+    cudaEvent_t a, b;
+  };
+  std::vector<TimedLaunch> ev_used;
   double t_ms[LGV_NKCLASS] = {0};
   int64_t t_n[LGV_NKCLASS] = {0};
   // differentiable Euler-Maruyama run (lgv_em_forward / lgv_em_backward)
@@ -191,9 +195,9 @@ cudaEvent_t pool_event(lgv_handle *h) {
 // timing is enabled; the events are resolved in lgv_timing_read.
 struct KTimer {
   lgv_handle *h;
-  int cls;
+  int cls, units;
   cudaEvent_t a = nullptr, b = nullptr;
-  KTimer(lgv_handle *hh, int c) : h(hh), cls(c) {
+  KTimer(lgv_handle *hh, int c, int u = 1) : h(hh), cls(c), units(u) {
     if (!h->timing_on) return;
     a = pool_event(h);
     b = pool_event(h);
@@ -202,7 +206,7 @@ struct KTimer {
   ~KTimer() {
     if (!a) return;
     cudaEventRecord(b, h->stream);
-    h->ev_used.push_back({cls, {a, b}});
+    h->ev_used.push_back({cls, units, a, b});
   }
 };
 
@@ -263,7 +267,7 @@ int sub_hb(lgv_handle *h, double dt, double mass) {  // EulerLangevinHB::step (S
     a.sk = lgv::sub_key(h->key, h->ctr);
   }
   if (h->hb_fused) {
-    KTimer tm(h, LGV_KCLASS_PHI_HB);
+    KTimer tm(h, LGV_KCLASS_PHI_HB, 2);  // one launch, both parity passes
     LGV_CK(lgv::launch_hb_sweep(h->cur, h->alt, h->N, a, h->stream));
     for (int l = 0; l < 4; ++l) std::swap(h->cur.c[l], h->alt.c[l]);
   } else {
@@ -325,7 +329,7 @@ int sub_charge(lgv_handle *h, double dt) {  // ModelGChargeHB::step (Stepper.cxx
         d.sk[i] = (h->noise_mode != LGV_NOISE_INJECTED) ? lgv::sub_key(h->key, h->ctr + 1 + 2 * ixyz + i) : 0;
       }
       bool swapped = false;
-      KTimer tm(h, LGV_KCLASS_CHARGE);
+      KTimer tm(h, LGV_KCLASS_CHARGE, 2);
       LGV_CK(lgv::launch_charge_dir(h->cur, h->alt, h->N, xyz[ixyz], d, h->stream, &swapped));
       if (swapped)
         for (int L = 4; L < 10; ++L) std::swap(h->cur.c[L], h->alt.c[L]);
@@ -477,8 +481,8 @@ int lgv_destroy(lgv_handle *h) {
     if (b) cudaFree(b);
   if (h->adj.done) cudaFree(h->adj.done);
   for (auto &u : h->ev_used) {
-    cudaEventDestroy(u.second.first);
-    cudaEventDestroy(u.second.second);
+    cudaEventDestroy(u.a);
+    cudaEventDestroy(u.b);
   }
   for (auto e : h->ev_pool) cudaEventDestroy(e);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
@@ -718,8 +722,8 @@ int lgv_timing_enable(lgv_handle *h, int enable) {
   DeviceGuard g(h->device);
   LGV_CK(cudaStreamSynchronize(h->stream));
   for (auto &u : h->ev_used) {
-    h->ev_pool.push_back(u.second.first);
-    h->ev_pool.push_back(u.second.second);
+    h->ev_pool.push_back(u.a);
+    h->ev_pool.push_back(u.b);
   }
   h->ev_used.clear();
   for (int c = 0; c < LGV_NKCLASS; ++c) {
@@ -737,11 +741,11 @@ int lgv_timing_read(lgv_handle *h, int kclass, double *total_ms, int64_t *launch
   LGV_CK(cudaStreamSynchronize(h->stream));
   for (auto &u : h->ev_used) {
     float ms = 0;
-    LGV_CK(cudaEventElapsedTime(&ms, u.second.first, u.second.second));
-    h->t_ms[u.first] += ms;
-    h->t_n[u.first] += 1;
-    h->ev_pool.push_back(u.second.first);
-    h->ev_pool.push_back(u.second.second);
+    LGV_CK(cudaEventElapsedTime(&ms, u.a, u.b));
+    h->t_ms[u.cls] += ms;
+    h->t_n[u.cls] += u.units;
+    h->ev_pool.push_back(u.a);
+    h->ev_pool.push_back(u.b);
   }
   h->ev_used.clear();
   *total_ms = h->t_ms[kclass];
