@@ -147,8 +147,8 @@ def computeBlockedOtOtp(arr1, arr2, nTMax, steps, decim=1, conn=False):
     a, was_np = _to_device(arr1)
     b, _ = _to_device(arr2)
     res = [_correlate(a[s:s + steps], b[s:s + steps], nTMax, decim, conn) for s in range(0, a.shape[0] - steps, steps)]
-    if not res:
-        raise ValueError("no complete block")
+    if not res:  # the reference returns an empty array
+        return _back(torch.empty(0, dtype=torch.float64, device=a.device), was_np)
     return _back(torch.stack(res), was_np)
 
 
@@ -162,7 +162,7 @@ def blockedOtOtp(arr1, arr2, nTMax, nblocks, decim=1):
     sMax = a.shape[0] - nTMax
     steps = int(sMax / nblocks)
     sMax = steps * nblocks
-    if steps < 1:
-        raise ValueError("blocks are empty")
+    if steps < 1:  # the reference's range() is empty (or its step zero, which raises)
+        raise ValueError("blocks are empty: len(arr1) - nTMax < nblocks")
     res = [_correlate(a[s:s + steps], b[s:s + steps], nTMax, decim, False) for s in range(0, sMax, steps)]
     return _back(torch.stack(res), was_np)
