@@ -285,6 +285,10 @@ int lgv_ensemble_tune(lgv_ensemble *e, int tile, int zchunk, int order);
  * fastest; choice[3] = (tile, zchunk, order), *ms_per_step its time */
 int lgv_ensemble_autotune(lgv_ensemble *e, int evolver, int inner, int outer, double dt, int steps, int *choice,
                           double *ms_per_step);
+/* CUDA-graph replay of lgv_ensemble_step (on by default): two steps are
+ * captured once per (evolver, inner, outer, dt, buffer phases) on the
+ * ensemble's own stream and replayed on its current stream, which may be any
+ * stream the caller set, the legacy default stream included. */
 int lgv_ensemble_use_graphs(lgv_ensemble *e, int enable);
 /* Differentiable Euler-Maruyama Model A runs of all replicas at once (no
  * counterpart in the reference): one launch per step over all replicas.
