@@ -5,7 +5,7 @@
 
 Workload: the full Model G step "PV2HBSplit23" (3 x [ideal PV2(dt/3) + 2 x phi
 heat bath(dt/6)] + charge heat bath(dt), Stepper.cxx:542-580) on a 256^3
-periodic FP64 lattice with the config-1 coefficients at H = 0.003 (m^2 = -4.813,
+periodic FP64 lattice with the heat-bath coefficients at H = 0.003 (m^2 = -4.813,
 lambda = 10, Gamma = 1, chi = 5, D = 1/3, dt = 0.04), measuring every 10 steps
 (saveFrequency, SuperPions.cxx:127-140).  Seeded synthetic state: phi ~
 0.1 N(0,1), charges ~ sqrt(chi) N(0,1) with the zero mode removed.  The state
@@ -240,7 +240,7 @@ def run_ensemble(steps=20, plain_steps=2):
     best_plain = min(plain.values())
     return {
         "workload": "PV2HBSplit23, 256 x 32^3 + 64 x 48^3 + 16 x 64^3 replicas, distinct seeds, "
-                    "H in (0.003, 0.006, 0.012) round robin, config-1 coefficients",
+                    "H in (0.003, 0.006, 0.012) round robin, m^2=-4.813, lambda=10, Gamma=1, chi=5, D=1/3",
         "replicas": R, "sites": sites,
         "batched_ms_per_step": ms, "batched_replica_steps_per_s": R / (ms / 1e3),
         "batched_site_updates_per_s": sites / (ms / 1e3),
@@ -253,11 +253,11 @@ def run_ensemble(steps=20, plain_steps=2):
     }
 
 
-CFG2 = dict(N=64, steps=10000, measure_every=10, mass0=-4.813, lam=10.0, H=0.006, chi=5.0, gamma=1.0,
-            diffusion=1.0 / 3.0, dt=0.04)
+MODEL_G_64 = dict(N=64, steps=10000, measure_every=10, mass0=-4.813, lam=10.0, H=0.006, chi=5.0, gamma=1.0,
+                  diffusion=1.0 / 3.0, dt=0.04)
 
 
-def run_config2():
+def run_model_g_64():
     """Full Model G on 64^3 with the (1, 1) composer (one ideal step, one phi
     heat-bath sweep, one charge heat bath per step), charges starting at 0, phi
     from N(0, 0.1^2), 10^4 steps with the full measurement (walls, phase walls,
@@ -272,7 +272,7 @@ def run_config2():
     from langevina_b200 import _lib as L
 
     lib = L.load()
-    c = CFG2
+    c = MODEL_G_64
     N, S, E = c["N"], c["steps"], c["measure_every"]
     V = N ** 3
     p = L.make_params(N, seed=2024, mass0=c["mass0"], lam=c["lam"], H=c["H"], chi=c["chi"], gamma=c["gamma"],
@@ -736,9 +736,9 @@ def run_ours(a):
     if world == 1 and not a.no_adjoint:
         adjoint = run_adjoint()
         adjoint["batched"] = run_adjoint_batch()
-    config2 = None
+    model_g_64 = None
     if world == 1 and not a.no_variants:
-        config2 = run_config2()
+        model_g_64 = run_model_g_64()
     postprocess = None
     if world == 1 and not a.no_postprocess:
         postprocess = run_postprocess()
@@ -763,7 +763,7 @@ def run_ours(a):
         "ensemble": ensemble,
         "adjoint": adjoint,
         "variants": variants,
-        "config2": config2,
+        "model_g_64cubed": model_g_64,
         "postprocess": postprocess,
         "gpu_launches": launches,
         "clocks": ck,

@@ -30,7 +30,7 @@ def _meas_close(gm, om, rtol, what):
         assert d <= rtol * scale, f"{what} {k}: {d:.3e}"
 
 
-def test_config1_model_a_1000_sweeps_injected(lgv, oracle_mod):
+def test_model_a_32cubed_1000_sweeps_injected(lgv, oracle_mod):
     from langevina_b200 import _lib as L
 
     N, seed = 32, 20240101
@@ -56,10 +56,10 @@ def test_config1_model_a_1000_sweeps_injected(lgv, oracle_mod):
             _meas_close(gm, om, 1e-11, f"sweep {sweep + 1}")
             kz = gm.wall_k[2][:, :17]  # z-axis modes k = 0..16 of the 11 observables
             assert kz.shape == (11, 17, 2) and np.all(np.isfinite(kz))
-    assert_state_close(g.get_state(), o.get_state(), rtol=1e-11, what="config 1 after 1000 sweeps")
+    assert_state_close(g.get_state(), o.get_state(), rtol=1e-11, what="32^3 Model A after 1000 sweeps")
 
 
-def test_config2_model_g_64cubed_counter(lgv, oracle_mod):
+def test_model_g_64cubed_counter(lgv, oracle_mod):
     from langevina_b200 import _lib as L
 
     N, seed = 64, 2024
@@ -81,5 +81,5 @@ def test_config2_model_g_64cubed_counter(lgv, oracle_mod):
             assert np.abs(gm.OAverage[7:10] * V).max() < 1e-10  # total vector charge stays 0
     assert g.counter() == o.get_counter()
     gs = g.get_state()
-    assert_state_close(gs, o.get_state(), rtol=1e-11, what="config 2 after 20 steps")
+    assert_state_close(gs, o.get_state(), rtol=1e-11, what="64^3 Model G after 20 steps")
     assert np.abs(gs[..., 7:10].sum(axis=(0, 1, 2))).max() < 1e-10
