@@ -585,8 +585,10 @@ __device__ __forceinline__ void charge_link_site(const Fields &f, const Geo &g, 
 }
 
 // Grid as hb_pass_kernel (pass_site).
+// 16 blocks of 128 threads per SM (32 registers): the link updates are long
+// integer / FP64 chains, and full occupancy hides them best
 template <bool INJECTED, bool MON, bool ROWS>
-__global__ void __launch_bounds__(128) charge_pass_kernel(Fields f, Geo g, int dir, int eoA, ChargeArgs a) {
+__global__ void __launch_bounds__(128, 16) charge_pass_kernel(Fields f, Geo g, int dir, int eoA, ChargeArgs a) {
   int m, j, k;
   MonLocal mon;
   if (pass_site<ROWS>(g, m, j, k)) charge_link_site<INJECTED, MON>(f, g, dir, eoA, a, m, j, k, mon);
@@ -1563,7 +1565,10 @@ __global__ void __launch_bounds__(128) batch_hb_kernel(const RepDesc *__restrict
   a.sk = sub_key(R.key, y.ctr + (unsigned long long)ctr_off);
   const Fields f = rep_fields(R, phase, phase);
   MonLocal mon;
-  for (int k = k0; k < min(k0 + kBatchPlanes, R.g.N); ++k) hb_site<false, false>(f, R.g, parity, a, m, j, k, mon);
+  // unrolled so the planes' loads and updates interleave (independent sites)
+#pragma unroll
+  for (int q = 0; q < kBatchPlanes; ++q)
+    if (k0 + q < R.g.N) hb_site<false, false>(f, R.g, parity, a, m, j, k0 + q, mon);
 }
 
 __global__ void __launch_bounds__(128) batch_charge_kernel(const RepDesc *__restrict__ d,
@@ -1594,8 +1599,9 @@ __global__ void __launch_bounds__(128) batch_charge_kernel(const RepDesc *__rest
   a.pass = pass;
   const Fields f = rep_fields(R, phase, phase);
   MonLocal mon;
-  for (int k = k0; k < min(k0 + kBatchPlanes, R.g.N); ++k)
-    charge_link_site<false, false>(f, R.g, dir, eoA, a, m, j, k, mon);
+#pragma unroll
+  for (int q = 0; q < kBatchPlanes; ++q)
+    if (k0 + q < R.g.N) charge_link_site<false, false>(f, R.g, dir, eoA, a, m, j, k0 + q, mon);
 }
 
 // ---- differentiable Euler-Maruyama runs of an ensemble ---------------------
