@@ -1571,7 +1571,8 @@ __global__ void __launch_bounds__(128) batch_hb_kernel(const RepDesc *__restrict
     if (k0 + q < R.g.N) hb_site<false, false>(f, R.g, parity, a, m, j, k0 + q, mon);
 }
 
-__global__ void __launch_bounds__(128) batch_charge_kernel(const RepDesc *__restrict__ d,
+// 32 registers, full occupancy (as charge_pass_kernel)
+__global__ void __launch_bounds__(128, 16) batch_charge_kernel(const RepDesc *__restrict__ d,
                                                            const EnsDyn *__restrict__ dyn, const int *__restrict__ rep,
                                                            const int *__restrict__ first, int phase, int pass,
                                                            double dt, int ctr_off_order) {
