@@ -146,3 +146,29 @@ def test_device_history_correlator(lgv):
     want, _ = P.computeOtOtp(dn, np.conj(dn), nTMax=50, conn=True)
     close(got.cpu().numpy(), want)
     g.close()
+
+
+def test_correlator_unaligned_complex_pairs(lgv):
+    """Complex series whose pairs do not start on 16 bytes (an 8-byte offset
+    into the buffer) take the kernel's two-load path; same results."""
+    import torch
+    from langevina_b200 import _lib as L
+
+    T, ns, ntmax = 90, 37, 31
+    rng = np.random.default_rng(8)
+    a = rng.normal(size=(T, ns)) + 1j * rng.normal(size=(T, ns))
+    b = rng.normal(size=(T, ns)) + 1j * rng.normal(size=(T, ns))
+    bufs = []
+    for x in (a, b):
+        t = torch.zeros(T * ns * 2 + 1, dtype=torch.float64, device="cuda")
+        t[1:].copy_(torch.from_numpy(np.ascontiguousarray(x).view(np.float64).ravel()))
+        bufs.append(t)
+    out = torch.zeros(ntmax * ns * 2 + 1, dtype=torch.float64, device="cuda")
+    lib = L.load()
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    L.check(lib.lgv_time_correlator(C.c_void_p(bufs[0].data_ptr() + 8), C.c_void_p(bufs[1].data_ptr() + 8), T, ns,
+                                    2 * ns, 1, ntmax, 1, 1, C.c_void_p(out.data_ptr() + 8), stream),
+            "lgv_time_correlator")
+    got = out[1:].cpu().numpy().view(np.complex128).reshape(ntmax, ns)
+    want, _ = P.computeOtOtp(a, b, conn=True, nTMax=ntmax)
+    close(got, want)
