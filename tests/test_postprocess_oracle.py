@@ -5,7 +5,9 @@
 - x2k on the test signal of ModelG/x2ktest.py (cos and sin of 2 pi k x / 8,
   k = 0, 1, 2): single modes of weight 1 (k = 0) or 1/2;
 - x2k_rotated known answers: for n = (1, 0, 0, 0) the rotated A and V rows are
-  (0, A_1..3) and (0, V_1..3), phi splits into its n part and the rest.
+  (0, A_1..3) and (0, V_1..3), phi splits into its n part and the rest;
+- both transforms reproduce the C++ oracle's measurer (its k walls and
+  rotated k walls) on a random lattice.
 """
 import importlib.util
 import json
@@ -109,3 +111,22 @@ def test_x2k_rotated_is_a_rotation_of_phi():
     # phi = n phis + phir with phir orthogonal to n
     assert np.allclose(n[:, :, None] * o[:, None, 0] + o[:, 1:5], c[:, 0:4])
     assert np.allclose(np.einsum("ra,rak->rk", n, o[:, 1:5]), 0)
+
+
+def test_restatements_agree_with_the_measurer_restatement(oracle_mod):
+    """x2k and x2k_rotated restated here reproduce the C++ oracle's measurer
+    (measurer.cxx: r2c walls / N and rotate_to_vev) on a random lattice."""
+    from langevina_b200 import _lib as L
+
+    N = 8
+    o = oracle_mod.Oracle(N, mode=oracle_mod.COUNTER, seed=5)
+    rng = np.random.default_rng(12)
+    u = np.zeros((N, N, N, 10))
+    u[..., :4] = 0.4 * rng.normal(size=(N, N, N, 4)) + np.array([0.5, 0.1, -0.2, 0.05])
+    u[..., 4:] = rng.normal(size=(N, N, N, 6))
+    o.set_state(u)
+    m = o.measure(L.Measurement(N))
+    for a in range(3):
+        assert np.allclose(P.x2k(m.wall[a]), m.wall_k[a], rtol=1e-12, atol=1e-14)
+        assert np.allclose(P.x2k(m.wall_phase[a]), m.wall_phase_k[a], rtol=1e-12, atol=1e-14)
+        assert np.allclose(P.x2k_rotated(m.wall_k[a][None])[0], m.wall_k_rotated[a][:13], rtol=1e-12, atol=1e-14)
