@@ -62,10 +62,11 @@ def x2k(walls):
     """W(k) = (1/N) sum_x W(x) e^{-2 pi i k x/N}, k = 0..N/2, over the last axis:
     [..., N] -> [..., N/2+1, 2] (x2k.cxx:94-113)."""
     torch = _torch()
+    complex_in = walls.is_complex() if isinstance(walls, torch.Tensor) else np.iscomplexobj(walls)
+    if complex_in:
+        raise ValueError("x2k transforms real walls (x2k.cxx reads real rows)")
     w, was_np = _to_device(walls)
-    if w.is_complex() or w.dtype != torch.float64:
-        w = w.to(torch.float64)
-    w = w.contiguous()
+    w = w.to(torch.float64).contiguous()
     N = w.shape[-1]
     rows = w.numel() // N if N else 0
     out = torch.empty(tuple(w.shape[:-1]) + (N // 2 + 1, 2), dtype=torch.float64, device=w.device)
