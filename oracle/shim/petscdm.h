@@ -1,0 +1,4 @@
+// petscdm.h -- TEST INFRASTRUCTURE ONLY: forwards to the DMDA layer of the oracle's
+// reference build.
+#pragma once
+#include "petscdmda.h"

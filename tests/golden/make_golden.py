@@ -14,7 +14,7 @@ hcrit1.json   -- equilibrium <phi_0> of the Model A heat bath read from
                  (parameters decoded from the file name: N=32, m^2=-4.813,
                  H=0.01, lambda=10).
 
-Usage:  python tests/golden/make_golden.py [--ref /root/reference/ModelG]
+Usage:  python tests/golden/make_golden.py --ref <reference ModelG directory>
 """
 import argparse
 import json
@@ -28,7 +28,7 @@ REPO = os.path.dirname(os.path.dirname(HERE))
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference/ModelG")
+    ap.add_argument("--ref", required=True, help="the reference's ModelG directory")
     a = ap.parse_args()
     subprocess.check_call(["make", "-C", os.path.join(REPO, "oracle"), "ref", f"REF={a.ref}"])
     out = subprocess.check_output([os.path.join(REPO, "oracle", "_ref", "ref_xoro")], text=True)

@@ -10,7 +10,7 @@ in sys.modules before the import.
 The inputs are not stored: tests rebuild them from the recorded seeds with
 series(seed, T, ncol, complex).
 
-Usage:  python tests/golden/make_postprocess_golden.py [--ref /root/reference/python]
+Usage:  python tests/golden/make_postprocess_golden.py --ref <reference python directory>
 """
 import argparse
 import importlib.util
@@ -44,7 +44,7 @@ def enc(a):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference/python")
+    ap.add_argument("--ref", required=True, help="the reference's python directory")
     a = ap.parse_args()
     sys.modules.setdefault("h5py", types.ModuleType("h5py"))
     spec = importlib.util.spec_from_file_location("reference_loader", os.path.join(a.ref, "Loader.py"))
