@@ -92,6 +92,20 @@ struct lgv_handle {
   // phi heat bath as one z-marching sweep kernel instead of two parity
   // passes (LGV_HB_FUSED=1 in the environment at lgv_create)
   bool hb_fused = false;
+  // phi sweeps as ordered persistent launches (hb_ordered_kernel), opt-in:
+  // LGV_HB_ORDERED=1 (=1,S,spc,lag,fuse also sets planes per slab, sites per
+  // chunk, schedule lag and how many consecutive sweeps share a launch).  On
+  // B200 at 256^3 the two one-parity launches are faster: the pass is near
+  // its instruction-issue limit, and at ~1300 resident CTAs the odd pass of a
+  // slab re-reads it from DRAM anyway (57.5 of 64 B/site per sweep measured)
+  bool hb_ordered = false;
+  int hb_fuse = 2;
+  lgv::HbPlan hb_plan;
+  // this handle's count of bounded device waits that gave up (TMA copies of
+  // the ideal step), and the polls before one gives up (LGV_WAIT_LIMIT at
+  // lgv_create; the default is lgv::kWaitLimit)
+  unsigned long long *waits_dev = nullptr;
+  int wait_limit = lgv::kWaitLimit;
   // charge heat bath as three two-face launches (one per direction) instead
   // of six single-face launches (LGV_CHARGE_FUSED=1 at lgv_create)
   bool charge_per_face = true;
@@ -138,11 +152,23 @@ int ensure(double **p, size_t n) {
   return LGV_OK;
 }
 
-// A bounded device wait (TMA completion) that gave up leaves a count behind:
-// report it once as an error.
-int check_waits() {
-  const unsigned n = lgv::read_wait_timeouts(true);
-  if (n) return fail(LGV_ERR_CUDA, "%u bounded device waits timed out (TMA copies did not complete)", n);
+// A bounded device wait that gave up -- a TMA copy of the ideal step, or an
+// ordered sweep's wait for the slabs it depends on -- leaves a count in this
+// handle's counters: report it once, as LGV_ERR_TIMEOUT.  Synchronises the
+// handle's stream.
+int check_waits(lgv_handle *h) {
+  unsigned long long n = 0, m = 0;
+  if (h->waits_dev) {
+    LGV_CK(cudaMemcpyAsync(&n, h->waits_dev, sizeof(n), cudaMemcpyDeviceToHost, h->stream));
+    LGV_CK(cudaStreamSynchronize(h->stream));
+    if (n) LGV_CK(cudaMemsetAsync(h->waits_dev, 0, sizeof(n), h->stream));
+  }
+  LGV_CK(lgv::hb_plan_timeouts(h->hb_plan, h->stream, &m, true));
+  if (n || m)
+    return fail(LGV_ERR_TIMEOUT,
+                "bounded device waits timed out: %llu TMA copy waits, %llu ordered-sweep dependency waits; the state "
+                "is not valid",
+                n, m);
   return LGV_OK;
 }
 
@@ -225,12 +251,14 @@ int energy_now(lgv_handle *h, double *E) {
 int sub_ideal(lgv_handle *h, double dt) {  // IdealPV2::step (Stepper.cxx:23-66)
   double Eold = 0, Enew = 0;
   if (h->mon_on) LGV_TRY(energy_now(h, &Eold));
-  lgv::IdealArgs a;
+  lgv::IdealArgs a{};
   a.dto2chi = (dt / 2.0) / h->p.chi;
   a.dt = dt;
   const double hx = h->p.LX / h->N;
   a.a2 = std::pow(1.0 / hx, 2);
   a.H = h->p.H;
+  a.waits = h->waits_dev;
+  a.wait_limit = h->wait_limit;
   {
     KTimer tm(h, LGV_KCLASS_IDEAL);
     LGV_CK(lgv::launch_ideal(h->cur, h->alt, h->N, a, h->stream));
@@ -266,7 +294,10 @@ int sub_hb(lgv_handle *h, double dt, double mass) {  // EulerLangevinHB::step (S
   } else {
     a.sk = lgv::sub_key(h->key, h->ctr);
   }
-  if (h->hb_fused) {
+  if (h->hb_ordered) {
+    KTimer tm(h, LGV_KCLASS_PHI_HB, 2);  // one launch, both parity passes
+    LGV_CK(lgv::launch_hb_ordered(h->cur, h->N, a, h->hb_plan, 1, nullptr, h->stream));
+  } else if (h->hb_fused) {
     KTimer tm(h, LGV_KCLASS_PHI_HB, 2);  // one launch, both parity passes
     LGV_CK(lgv::launch_hb_sweep(h->cur, h->alt, h->N, a, h->stream));
     for (int l = 0; l < 4; ++l) std::swap(h->cur.c[l], h->alt.c[l]);
@@ -278,6 +309,36 @@ int sub_hb(lgv_handle *h, double dt, double mass) {  // EulerLangevinHB::step (S
   }
   if (h->noise_mode == LGV_NOISE_INJECTED) h->have_hb = false;
   else h->ctr += 1;
+  return LGV_OK;
+}
+
+// n consecutive heat-bath sweeps (the inner loop of PV2HBSplit::step,
+// Stepper.cxx:562-564).  With counter noise and no per-site flags, up to
+// hb_fuse of them share one ordered launch: sweep q draws with counter
+// ctr + q, exactly as n separate sweeps do.
+int sub_hb_n(lgv_handle *h, double dt, double mass, int n) {
+  if (!h->hb_ordered || h->noise_mode != LGV_NOISE_COUNTER || h->flags_dev || h->hb_fuse < 2 || n < 2) {
+    for (int i = 0; i < n; ++i) LGV_TRY(sub_hb(h, dt, mass));
+    return LGV_OK;
+  }
+  lgv::HbArgs a{};
+  a.rdtg = std::sqrt(2. * dt * h->p.gamma);
+  a.Lambda2 = 0.5 * (2. * 3. + mass);
+  a.lam4 = h->p.lambda / 4.;
+  a.H = h->p.H;
+  a.mon = mon_ptr(h, LGV_MONITOR_PHI_HB);
+  for (int done = 0; done < n;) {
+    const int k = std::min(n - done, std::min(h->hb_fuse, lgv::kHbMaxSweeps));
+    uint64_t sk[lgv::kHbMaxSweeps];
+    for (int q = 0; q < k; ++q) sk[q] = lgv::sub_key(h->key, h->ctr + q);
+    a.sk = sk[0];
+    {
+      KTimer tm(h, LGV_KCLASS_PHI_HB, 2 * k);
+      LGV_CK(lgv::launch_hb_ordered(h->cur, h->N, a, h->hb_plan, k, sk, h->stream));
+    }
+    h->ctr += k;
+    done += k;
+  }
   return LGV_OK;
 }
 
@@ -372,7 +433,7 @@ int step_once(lgv_handle *h, int ev, int inner, int outer, double dt, double t) 
       if (ev != LGV_PV2HBSPLIT_ONLYDIFFUSE) {
         for (int i1 = 0; i1 < outer; ++i1) {
           LGV_TRY(sub_ideal(h, dt / (unsigned)outer));
-          for (int i0 = 0; i0 < inner; ++i0) LGV_TRY(sub_hb(h, dt / ((unsigned)inner * (unsigned)outer), mass));
+          LGV_TRY(sub_hb_n(h, dt / ((unsigned)inner * (unsigned)outer), mass, inner));
         }
       }
       if (ev != LGV_PV2HBSPLIT_NODIFFUSE) LGV_TRY(sub_charge(h, dt));
@@ -439,6 +500,20 @@ int lgv_create(const lgv_params *params, lgv_handle **out) {
     const char *c = std::getenv("LGV_CHARGE_FUSED");
     h->charge_per_face = !(c && c[0] == '1');
   }
+  int hb_slab = 4, hb_spc = 1024, hb_lag = 2;
+  {
+    const char *o = std::getenv("LGV_HB_ORDERED");
+    h->hb_ordered = false;
+    if (o && o[0]) {
+      int on = 1, fuse = h->hb_fuse;
+      std::sscanf(o, "%d,%d,%d,%d,%d", &on, &hb_slab, &hb_spc, &hb_lag, &fuse);
+      h->hb_ordered = on != 0;
+      h->hb_fuse = fuse;
+    }
+    if (h->hb_fused) h->hb_ordered = false;
+    const char *wl = std::getenv("LGV_WAIT_LIMIT");
+    if (wl && wl[0]) h->wait_limit = std::max(0, std::atoi(wl));
+  }
   int rc = LGV_OK;
   if (cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
     rc = fail(LGV_ERR_CUDA, "cudaStreamCreate failed");
@@ -458,6 +533,16 @@ int lgv_create(const lgv_params *params, lgv_handle **out) {
         cudaMemsetAsync(h->mon_dev, 0, 3 * sizeof(lgv::MonAcc), h->stream) != cudaSuccess ||
         cudaStreamSynchronize(h->stream) != cudaSuccess)
       rc = fail(LGV_ERR_CUDA, "initial memset failed");
+  }
+  if (rc == LGV_OK) {
+    if (cudaMalloc((void **)&h->waits_dev, sizeof(unsigned long long)) != cudaSuccess ||
+        cudaMemset(h->waits_dev, 0, sizeof(unsigned long long)) != cudaSuccess)
+      rc = fail(LGV_ERR_NOMEM, "wait counter alloc failed");
+  }
+  if (rc == LGV_OK && h->hb_ordered) {
+    h->hb_plan.wait_limit = h->wait_limit;
+    const cudaError_t e = lgv::hb_plan_build(h->hb_plan, h->N, hb_slab, hb_spc, hb_lag);
+    if (e != cudaSuccess) rc = fail(LGV_ERR_CUDA, "ordered sweep plan: %s", cudaGetErrorString(e));
   }
   if (rc != LGV_OK) {
     lgv_destroy(h);
@@ -480,6 +565,8 @@ int lgv_destroy(lgv_handle *h) {
   for (double *b : {h->adj.ckpt, h->adj.seg, h->adj.lam, h->adj.work, h->adj.avg_dev, h->adj.partial, h->adj.g4})
     if (b) cudaFree(b);
   if (h->adj.done) cudaFree(h->adj.done);
+  lgv::hb_plan_free(h->hb_plan);
+  if (h->waits_dev) cudaFree(h->waits_dev);
   for (auto &u : h->ev_used) {
     cudaEventDestroy(u.a);
     cudaEventDestroy(u.b);
@@ -516,7 +603,7 @@ int lgv_get_state(lgv_handle *h, double *host_aos) {
   LGV_CK(lgv::launch_rb_to_aos(h->cur, h->staging, h->N, h->stream));
   LGV_CK(cudaMemcpyAsync(host_aos, h->staging, 10 * h->V * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   LGV_CK(cudaStreamSynchronize(h->stream));
-  return check_waits();
+  return check_waits(h);
 }
 
 int lgv_set_state_device(lgv_handle *h, const double *dev_aos) {
@@ -714,7 +801,7 @@ int lgv_synchronize(lgv_handle *h) {
   if (!h) return fail(LGV_ERR_INVALID, "handle is NULL");
   DeviceGuard g(h->device);
   LGV_CK(cudaStreamSynchronize(h->stream));
-  return check_waits();
+  return check_waits(h);
 }
 
 int lgv_timing_enable(lgv_handle *h, int enable) {
@@ -801,13 +888,15 @@ lgv::EmArgs em_args(const lgv_params &p, uint64_t key, uint64_t ctr, double dt, 
 }
 
 // arguments of an ideal step of size dt, as sub_ideal builds them
-lgv::IdealArgs ideal_args(const lgv_params &p, int N, double dt) {
+lgv::IdealArgs ideal_args(const lgv_params &p, int N, double dt, const lgv_handle *h) {
   lgv::IdealArgs a{};
   a.dto2chi = (dt / 2.0) / p.chi;
   a.dt = dt;
   const double hx = p.LX / N;
   a.a2 = std::pow(1.0 / hx, 2);
   a.H = p.H;
+  a.waits = h->waits_dev;
+  a.wait_limit = h->wait_limit;
   return a;
 }
 
@@ -847,7 +936,7 @@ int lgv_diff_forward(lgv_handle *h, int evolver, double dt, double t, int nsteps
   A.tn.assign(S + 1, 0.0);
   A.tn[0] = t;
   for (int n = 0; n < S; ++n) A.tn[n + 1] = A.tn[n] + dt;
-  const lgv::IdealArgs ia = ideal_args(A.p, h->N, dt);
+  const lgv::IdealArgs ia = ideal_args(A.p, h->N, dt, h);
   LGV_CK(lgv::launch_phi_avg(h->cur, h->N, A.partial, A.done, A.avg_dev, h->stream));
   for (int n = 0; n < S; ++n) {
     if (n % K == 0)
@@ -919,7 +1008,7 @@ int lgv_diff_backward(lgv_handle *h, const double *w, double *grad) {
     out[0] = w[0] / (Vd * M);
     for (int a = 1; a < 4; ++a) out[a] = w[1] * 2.0 * av[a] / M;
   };
-  const lgv::IdealArgs ia = ideal_args(A.p, N, A.dt);
+  const lgv::IdealArgs ia = ideal_args(A.p, N, A.dt, h);
   lgv::IdealAdjArgs iadj{};
   iadj.k = ia.dto2chi;
   iadj.dt = ia.dt;

@@ -76,6 +76,10 @@ struct lgv_ensemble {
   int tile = LGV_TILE_32x8, zchunk = 16, order = LGV_PACK_GIVEN;
   bool graphs = true;
   std::map<std::tuple<int, int, int, double, int, int>, cudaGraphExec_t> cache;
+  // bounded device waits of this ensemble's TMA ideal launches that gave up,
+  // and the polls before one gives up (LGV_WAIT_LIMIT at creation)
+  unsigned long long *waits = nullptr;
+  int wait_limit = lgv::kWaitLimit;
   // differentiable Euler-Maruyama run (lgv_ensemble_diff_forward / _backward)
   struct {
     bool ready = false;
@@ -95,6 +99,22 @@ struct lgv_ensemble {
 };
 
 namespace {
+
+// After a stream synchronisation: a bounded wait that gave up in this
+// ensemble's launches is reported once, as LGV_ERR_TIMEOUT (the states of the
+// replicas it touched are not valid).
+int ens_check_waits(lgv_ensemble *e) {
+  unsigned long long n = 0;
+  if (!e->waits) return LGV_OK;
+  ECK(cudaMemcpyAsync(&n, e->waits, sizeof(n), cudaMemcpyDeviceToHost, e->stream));
+  ECK(cudaStreamSynchronize(e->stream));
+  if (n) {
+    ECK(cudaMemsetAsync(e->waits, 0, sizeof(n), e->stream));
+    return efail(LGV_ERR_TIMEOUT, "bounded device waits timed out: " + std::to_string(n) +
+                                      " TMA copy waits of the ideal step; the ensemble state is not valid");
+  }
+  return LGV_OK;
+}
 
 void free_map(BlockMap &m) {
   if (m.rep) cudaFree(m.rep);
@@ -234,7 +254,7 @@ int enqueue_step(lgv_ensemble *e, int ev, int inner, int outer, double dt) {
   auto ideal = [&](double d) -> int {
     if (e->tma_map.nblocks > 0)
       ECK(lgv::launch_batch_ideal_tma(e->dd, e->gmaps, e->tma_map.rep, e->tma_map.first, e->tma_map.nblocks,
-                                      e->phase_phi, e->phase_q, d, e->stream));
+                                      e->phase_phi, e->phase_q, d, e->waits, e->wait_limit, e->stream));
     if (nb_i > 0)
       ECK(lgv::launch_batch_ideal(e->dd, e->ideal_map.rep, e->ideal_map.first, nb_i, e->tile, e->phase_phi,
                                   e->phase_q, d, e->stream));
@@ -321,6 +341,13 @@ int lgv_ensemble_create(int nrep, const lgv_params *params, lgv_ensemble **out) 
   if (cudaStreamCreateWithFlags(&e->own, cudaStreamNonBlocking) != cudaSuccess)
     return bail(efail(LGV_ERR_CUDA, "stream"));
   e->stream = e->own;
+  {
+    const char *wl = std::getenv("LGV_WAIT_LIMIT");
+    if (wl && wl[0]) e->wait_limit = std::max(0, std::atoi(wl));
+  }
+  if (cudaMalloc((void **)&e->waits, sizeof(unsigned long long)) != cudaSuccess ||
+      cudaMemset(e->waits, 0, sizeof(unsigned long long)) != cudaSuccess)
+    return bail(efail(LGV_ERR_NOMEM, "wait counter"));
   e->hd.resize(nrep);
   for (int r = 0; r < nrep; ++r) {
     const lgv_params &q = params[r];
@@ -378,6 +405,7 @@ int lgv_ensemble_destroy(lgv_ensemble *e) {
   if (e->diff.wg) cudaFree(e->diff.wg);
   if (e->diff.partial) cudaFree(e->diff.partial);
   if (e->diff.done) cudaFree(e->diff.done);
+  if (e->waits) cudaFree(e->waits);
   if (e->own) cudaStreamDestroy(e->own);
   delete e;
   return LGV_OK;
@@ -418,7 +446,7 @@ int lgv_ensemble_get_state(lgv_ensemble *e, int r, double *host_aos) {
   ECK(c1);
   ECK(c2);
   ECK(c3);
-  return LGV_OK;
+  return ens_check_waits(e);
 }
 
 int lgv_ensemble_initialize(lgv_ensemble *e, int kind, double scale) {
@@ -600,7 +628,7 @@ int lgv_ensemble_diff_forward(lgv_ensemble *e, double dt, double t, int nsteps, 
     obs[2 * r + 1] = o1 / (double)(S - avg_begin);
   }
   D.ready = true;
-  return LGV_OK;
+  return ens_check_waits(e);
 }
 
 int lgv_ensemble_diff_backward(lgv_ensemble *e, const double *w, double *grad) {
@@ -629,7 +657,7 @@ int lgv_ensemble_diff_backward(lgv_ensemble *e, const double *w, double *grad) {
   }
   ECK(cudaMemcpyAsync(grad, D.wg + 2 * R, (size_t)R * 4 * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
   ECK(cudaStreamSynchronize(e->stream));
-  return LGV_OK;
+  return ens_check_waits(e);
 }
 
 int lgv_ensemble_oaverage_device(lgv_ensemble *e, double *dev_out) {
@@ -646,7 +674,7 @@ int lgv_ensemble_oaverage(lgv_ensemble *e, double *host_out) {
   ETRY(lgv_ensemble_oaverage_device(e, e->oavg));
   ECK(cudaMemcpyAsync(host_out, e->oavg, (size_t)e->R * 11 * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
   ECK(cudaStreamSynchronize(e->stream));
-  return LGV_OK;
+  return ens_check_waits(e);
 }
 
 int lgv_ensemble_tune(lgv_ensemble *e, int tile, int zchunk, int order) {
@@ -767,7 +795,7 @@ int lgv_ensemble_set_stream(lgv_ensemble *e, void *s) {
 int lgv_ensemble_synchronize(lgv_ensemble *e) {
   if (!e) return efail(LGV_ERR_INVALID, "ensemble is NULL");
   ECK(cudaStreamSynchronize(e->stream));
-  return LGV_OK;
+  return ens_check_waits(e);
 }
 
 }  // extern "C"

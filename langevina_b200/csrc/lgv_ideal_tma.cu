@@ -26,9 +26,6 @@
 
 namespace lgv {
 
-// bounded waits that gave up (read and cleared by the host)
-__device__ unsigned g_wait_timeouts = 0;
-
 namespace {
 
 constexpr int TX = 32, TY = 8, NT = TX * TY;
@@ -78,11 +75,11 @@ __device__ __forceinline__ bool mbar_try(unsigned bar, unsigned parity) {
 }
 
 // Bounded wait for the phase `parity` of an mbarrier: false (and a count in
-// g_wait_timeouts) when it gives up.
-__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
-  for (int i = 0; i < (1 << 22); ++i)
+// *waits) when it gives up after `limit` polls.
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, int limit, unsigned long long *waits) {
+  for (int i = 0; i < limit; ++i)
     if (mbar_try(bar, parity)) return true;
-  atomicAdd(&g_wait_timeouts, 1u);
+  if (waits) atomicAdd(waits, 1ull);
   return false;
 }
 
@@ -167,7 +164,7 @@ __device__ __forceinline__ void ideal_tma_cta(const CUtensorMap *maps, const Fie
     wbar = bar0 + 8 * st;
     wpar = (unsigned)((it / NS) & 1);
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-    if (!mbar_wait(wbar, wpar)) s_abort = 1;
+    if (!mbar_wait(wbar, wpar, a.wait_limit, a.waits)) s_abort = 1;
     __syncthreads();
     if (s_abort) break;
     if (it + NS - 1 < nit) issue(it + NS - 1);  // its stage was last read in iteration it - 1
@@ -241,9 +238,10 @@ __device__ __forceinline__ void ideal_tma_cta(const CUtensorMap *maps, const Fie
     for (int s = 0; s < 6; ++s) qc[s] = qn[s];
   }
   if (s_abort) {
-    // the plane that timed out may still be in flight: one more bounded wait before the CTA retires
+    // the plane that timed out may still be in flight: one more bounded wait
+    // (the full limit, whatever the first one had) before the CTA retires
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-    if (tid == 0) mbar_wait(wbar, wpar);
+    if (tid == 0) mbar_wait(wbar, wpar, kWaitLimit, a.waits);
     __syncthreads();
   }
 }
@@ -260,7 +258,8 @@ __global__ void __launch_bounds__(NT, 2)
 // tensor-map proxy reads them.
 __global__ void __launch_bounds__(NT, 2)
     batch_ideal_tma_kernel(const RepDesc *__restrict__ d, const CUtensorMap *__restrict__ gmaps,
-                           const int *__restrict__ rep, const int *__restrict__ first, int pphi, int pq, double dt) {
+                           const int *__restrict__ rep, const int *__restrict__ first, int pphi, int pq, double dt,
+                           unsigned long long *waits, int wait_limit) {
   const int r = rep[blockIdx.x];
   const RepDesc &R = d[r];
   const int l = blockIdx.x - first[r];
@@ -283,6 +282,8 @@ __global__ void __launch_bounds__(NT, 2)
   a.dt = dt;
   a.a2 = R.a2;
   a.H = R.H;
+  a.waits = waits;
+  a.wait_limit = wait_limit;
   ideal_tma_cta(maps, in, out, R.g, R.izc, a, bx, by, bz);
 }
 
@@ -358,23 +359,14 @@ bool tma_plane_map(const double *plane, int N, void *out128) {
 }
 
 cudaError_t launch_batch_ideal_tma(const RepDesc *d, const void *gmaps, const int *rep, const int *first, int nblocks,
-                                   int phase_phi, int phase_q, double dt, cudaStream_t st) {
+                                   int phase_phi, int phase_q, double dt, unsigned long long *waits, int wait_limit,
+                                   cudaStream_t st) {
   cudaError_t e = cudaFuncSetAttribute(batch_ideal_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)kSmemBytes);
   if (e != cudaSuccess) return e;
   batch_ideal_tma_kernel<<<nblocks, NT, kSmemBytes, st>>>(d, reinterpret_cast<const CUtensorMap *>(gmaps), rep, first,
-                                                          phase_phi, phase_q, dt);
+                                                          phase_phi, phase_q, dt, waits, wait_limit);
   return cudaGetLastError();
-}
-
-unsigned read_wait_timeouts(bool clear) {
-  unsigned v = 0;
-  cudaMemcpyFromSymbol(&v, g_wait_timeouts, sizeof(v));
-  if (clear && v) {
-    const unsigned z = 0;
-    cudaMemcpyToSymbol(g_wait_timeouts, &z, sizeof(z));
-  }
-  return v;
 }
 
 }  // namespace lgv

@@ -66,7 +66,15 @@ struct IdealArgs {
   double dt;
   double a2;       // (1 / h)^2
   double H;
+  // Bounded device waits (TMA completion): a wait gives up after wait_limit
+  // polls and counts itself in *waits, the owning handle's or ensemble's
+  // counter, which the host reads at its next synchronising call.
+  unsigned long long *waits;
+  int wait_limit;
 };
+
+// Polls before a bounded device wait gives up (a few seconds at most).
+constexpr int kWaitLimit = 1 << 22;
 
 // ---------------------------------------------------------------------------
 // Batched ensembles: many independent lattices advanced by one launch per
@@ -188,6 +196,28 @@ cudaError_t launch_init_charges(Fields f, int N, uint64_t sk, double sqrtchi, do
                                 cudaStream_t st);
 // one phi heat-bath parity pass, in place
 cudaError_t launch_hb_pass(Fields f, int N, int parity, const HbArgs &a, cudaStream_t st);
+// Ordered phi sweeps (hb_ordered_kernel): one persistent launch runs 1 ..
+// kHbMaxSweeps whole sweeps in place, z-slab by z-slab.  A plan holds the
+// chunk schedule for each sweep count and the launch's counters; it is built
+// once per lattice size (device allocations) and used by one stream at a time.
+constexpr int kHbMaxSweeps = 4;
+struct HbPlan {
+  int N = 0, S = 0, nslab = 0, spc = 0, cpi = 0, grid = 0;
+  int *sched[kHbMaxSweeps] = {};
+  int total[kHbMaxSweeps] = {};
+  unsigned long long *sync = nullptr;
+  int wait_limit = kWaitLimit;  // polls before a dependency wait gives up
+};
+// slab_target: planes per slab at most; spc: sites per chunk (multiple of
+// 128); lag: schedule rounds between an item and its dependants
+cudaError_t hb_plan_build(HbPlan &plan, int N, int slab_target, int spc, int lag);
+void hb_plan_free(HbPlan &plan);
+// nsweeps sweeps with counter keys sk[0..nsweeps) (null: a.sk, one sweep);
+// injected noise and per-site flags allow one sweep per launch
+cudaError_t launch_hb_ordered(Fields f, int N, const HbArgs &a, const HbPlan &plan, int nsweeps, const uint64_t *sk,
+                              cudaStream_t st);
+// bounded waits of the plan's launches that gave up (synchronises `st`)
+cudaError_t hb_plan_timeouts(const HbPlan &plan, cudaStream_t st, unsigned long long *out, bool clear);
 // one full phi heat-bath sweep (both parities, z-marching): reads phi of `in`, writes phi of `out`
 cudaError_t launch_hb_sweep(Fields in, Fields out, int N, const HbArgs &a, cudaStream_t st);
 cudaError_t launch_charge_pass(Fields f, int N, int dir, int eoA, const ChargeArgs &a, cudaStream_t st);
@@ -210,9 +240,8 @@ cudaError_t launch_ideal_tma(Fields in, Fields out, int N, int zchunk, const Ide
 bool tma_plane_map(const double *plane, int N, void *out128);
 int batch_tma_blocks(int N, int zchunk);
 cudaError_t launch_batch_ideal_tma(const RepDesc *d, const void *gmaps, const int *rep, const int *first, int nblocks,
-                                   int phase_phi, int phase_q, double dt, cudaStream_t st);
-// bounded device waits that gave up since the last clear
-unsigned read_wait_timeouts(bool clear);
+                                   int phase_phi, int phase_q, double dt, unsigned long long *waits, int wait_limit,
+                                   cudaStream_t st);
 // energy: writes E into dev_out[0]; scratch >= energy_scratch_doubles(N)
 size_t energy_scratch_doubles(int N);
 cudaError_t launch_energy(Fields f, int N, double H, double inv2chi_half, double *scratch, double *dev_out,

@@ -28,6 +28,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
+#include <vector>
 
 namespace lgv {
 
@@ -309,7 +310,16 @@ __device__ __forceinline__ void mon_count(MonLocal &m, const HbDecision &d) {
 // Stepper.cxx:325-381).  One thread per site of `parity`: element m of the
 // parity half-row (j, k); its six neighbours are elements of the other
 // parity's half-rows.
-template <bool INJECTED, bool MON>
+// CG: phi is read at L2 (ld.global.cg), never from a possibly stale L1 line;
+// the ordered sweep (hb_ordered_kernel) reads sites other CTAs of the same
+// launch have just written.
+template <bool CG>
+__device__ __forceinline__ double ld_phi(const double *p) {
+  if (CG) return __ldcg(p);
+  return *p;
+}
+
+template <bool INJECTED, bool MON, bool CG = false>
 __device__ __forceinline__ void hb_site(const Fields &f, const Geo &g, int parity, const HbArgs &a, int m, int j,
                                         int k, MonLocal &mon) {
   const int H = g.H, N = g.N;
@@ -328,9 +338,10 @@ __device__ __forceinline__ void hb_site(const Fields &f, const Geo &g, int parit
 #pragma unroll
   for (int l = 0; l < 4; ++l) {
     const double *P = f.c[l];
-    heff[l] = (P[ob + row + xp] + P[ob + row + xm]) + (P[ob + rjp + m] + P[ob + rjm + m]) +
-              (P[ob + rkp + m] + P[ob + rkm + m]);
-    po[l] = P[own];
+    heff[l] = (ld_phi<CG>(P + ob + row + xp) + ld_phi<CG>(P + ob + row + xm)) +
+              (ld_phi<CG>(P + ob + rjp + m) + ld_phi<CG>(P + ob + rjm + m)) +
+              (ld_phi<CG>(P + ob + rkp + m) + ld_phi<CG>(P + ob + rkm + m));
+    po[l] = ld_phi<CG>(P + own);
   }
   const long long nat = ((long long)k * N + j) * N + 2 * m + s;
   HbDecision d;
@@ -374,6 +385,135 @@ __global__ void __launch_bounds__(128) hb_pass_kernel(Fields f, Geo g, int parit
   MonLocal mon;
   if (pass_site<ROWS>(g, m, j, k)) hb_site<INJECTED, MON>(f, g, parity, a, m, j, k, mon);
   if (MON) mon_flush(mon, a.mon);
+}
+
+// ----------------------------------------------------------------------------
+// Phi heat bath, one or more whole sweeps (EulerLangevinHB::step,
+// Stepper.cxx:287-389) in one persistent launch, ordered through the lattice
+// by z-slabs so that the odd pass of a slab runs while its phi is still in
+// L2.
+//
+// The lattice is cut into nslab slabs of S planes.  An item is one parity
+// pass (phase p: sweep p/2, parity p&1) over one slab; it is split into cpi
+// chunks of `spc` sites (sites of that parity in slab-local (k, j, m) order).
+// A host-built schedule lists every chunk of every item in an order in which
+// item (p, s) comes after the three items (p-1, s-1), (p-1, s), (p-1, s+1)
+// (periodic in s) it depends on: the pass of phase p reads the sites of the
+// other parity in planes sS-1 .. (s+1)S, which those items write, and writes
+// sites those items read.  CTAs draw chunks in schedule order from an atomic
+// ticket; a chunk of phase p >= 1 first waits until its three items have
+// completed all their chunks.  Chunks are only ever handed to running CTAs
+// and a chunk waits only on chunks with lower tickets, so the waits always
+// end; each is still bounded, and a wait that gives up counts in
+// sync[kSyncTimeouts], skips its sites and lets the host report
+// LGV_ERR_TIMEOUT.  The result is that of the sequential passes bit for bit:
+// every site sees exactly the neighbour values it sees there.
+//
+// phi moves 32 B/site in and 32 B/site out per sweep when the odd pass of a
+// slab re-reads it from L2 (the two one-parity launches move 48 B/site each).
+constexpr int kSyncTicket = 0, kSyncExit = 1, kSyncTimeouts = 2, kSyncDone = 3;
+constexpr int kHbOrderedThreads = 128;
+
+struct HbSched {
+  const int *sched;            // ticket -> item * cpi + chunk, item = phase * nslab + slab
+  unsigned long long *sync;    // [ticket, exits, timeouts, done[nphase * nslab]]
+  int total;                   // tickets
+  int cpi;                     // chunks per item
+  int spc;                     // sites per chunk (a multiple of kHbOrderedThreads)
+  int nslab, S, nphase;
+  int limit;                   // polls before a dependency wait gives up
+  uint64_t sk[4];              // counter keys of the sweeps (phase / 2)
+};
+
+__device__ __forceinline__ unsigned long long ld_acquire(const unsigned long long *p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];\n" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Thread 0 waits until the three items item (p, s) depends on have completed
+// all their chunks; false (and a count in sync[kSyncTimeouts]) if a wait gives
+// up.  `seen` caches the last two items already found ready.
+__device__ __forceinline__ bool hb_deps_ready(const HbSched &s, int item, int (&seen)[2]) {
+  const int phase = item / s.nslab, slab = item - phase * s.nslab;
+  if (phase == 0 || item == seen[0] || item == seen[1]) return true;
+  for (int d = -1; d <= 1; ++d) {
+    const int dep = (phase - 1) * s.nslab + (slab + d + s.nslab) % s.nslab;
+    const unsigned long long *p = &s.sync[kSyncDone + dep];
+    int it = 0;
+    while (ld_acquire(p) < (unsigned long long)s.cpi) {
+      if (++it > s.limit) {
+        atomicAdd(&s.sync[kSyncTimeouts], 1ull);
+        return false;
+      }
+      __nanosleep(64);
+    }
+  }
+  seen[1] = seen[0];
+  seen[0] = item;
+  return true;
+}
+
+template <bool INJECTED, bool MON>
+__global__ void __launch_bounds__(kHbOrderedThreads) hb_ordered_kernel(Fields f, Geo g, HbArgs a, HbSched s) {
+  __shared__ int s_work, s_ok;
+  MonLocal mon;
+  const long long item_sites = (long long)s.S * g.N * g.H;
+  // Thread 0 draws the next ticket while the CTA works on the current chunk.
+  // A CTA then holds at most two tickets, and each waits only on lower ones,
+  // so the lowest unfinished chunk can always proceed.
+  unsigned long long next = 0;
+  int seen[2] = {-1, -1};
+  if (threadIdx.x == 0) next = atomicAdd(&s.sync[kSyncTicket], 1ull);
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const int w = next < (unsigned long long)s.total ? __ldg(s.sched + next) : -1;
+      s_ok = w >= 0 ? (int)hb_deps_ready(s, w / s.cpi, seen) : 1;
+      s_work = w;
+    }
+    __syncthreads();
+    const int w = s_work, ok = s_ok;
+    if (w < 0) break;
+    if (threadIdx.x == 0) next = atomicAdd(&s.sync[kSyncTicket], 1ull);
+    const int item = w / s.cpi, chunk = w - item * s.cpi;
+    const int phase = item / s.nslab, slab = item - phase * s.nslab;
+    if (ok) {
+      HbArgs aa = a;
+      if (!INJECTED) {
+        const int q = phase >> 1;  // constant indices: the key array stays in kernel parameters
+        aa.sk = q == 0 ? s.sk[0] : q == 1 ? s.sk[1] : q == 2 ? s.sk[2] : s.sk[3];
+      }
+      const int parity = phase & 1;
+      for (int r = threadIdx.x; r < s.spc; r += kHbOrderedThreads) {
+        const long long q = (long long)chunk * s.spc + r;
+        if (q >= item_sites) break;
+        const unsigned u = (unsigned)q, H = (unsigned)g.H, N = (unsigned)g.N;
+        const unsigned row = u / H;
+        const int m = (int)(u - row * H);
+        const unsigned kk = row / N;
+        const int j = (int)(row - kk * N);
+        hb_site<INJECTED, MON, true>(f, g, parity, aa, m, j, slab * s.S + (int)kk, mon);
+      }
+    }
+    // The barrier orders every thread's stores before thread 0's fence, and
+    // the fence (cumulative) before the completion count.
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      atomicAdd(&s.sync[kSyncDone + item], 1ull);
+    }
+  }
+  if (MON) mon_flush(mon, a.mon);
+  // The last CTA out clears the ticket, exit and completion counters for the
+  // next launch (the timeout count stays for the host to read).
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(&s.sync[kSyncExit], 1ull) == gridDim.x - 1) {
+      s.sync[kSyncTicket] = 0;
+      s.sync[kSyncExit] = 0;
+      for (int i = 0; i < s.nphase * s.nslab; ++i) s.sync[kSyncDone + i] = 0;
+    }
+  }
 }
 
 // ----------------------------------------------------------------------------
@@ -2101,6 +2241,118 @@ cudaError_t launch_hb_pass(Fields f, int N, int parity, const HbArgs &a, cudaStr
   else { if (mon) { LGV_HBP(false, true); } else { LGV_HBP(false, false); } }
 #undef LGV_HBP
   return cudaGetLastError();
+}
+
+// ---- ordered sweeps ---------------------------------------------------------
+// Slab thickness: the largest divisor of N not above `target` that leaves at
+// least three slabs (an item depends on three distinct neighbours).
+static int hb_slab_planes(int N, int target) {
+  for (int S = std::min(target, N / 3); S >= 1; --S)
+    if (N % S == 0) return S;
+  return 0;
+}
+
+cudaError_t hb_plan_build(HbPlan &pl, int N, int slab_target, int spc, int lag) {
+  hb_plan_free(pl);
+  const int S = hb_slab_planes(N, slab_target);
+  if (S < 1 || spc < kHbOrderedThreads || spc % kHbOrderedThreads || lag < 1) return cudaErrorInvalidValue;
+  pl.N = N;
+  pl.S = S;
+  pl.nslab = N / S;
+  pl.spc = spc;
+  const long long item_sites = (long long)S * N * (N / 2);
+  pl.cpi = (int)((item_sites + spc - 1) / spc);
+  const int n = pl.nslab;
+  cudaError_t e;
+  for (int ns = 1; ns <= kHbMaxSweeps; ++ns) {
+    // T(0, s) = s; T(p, s) = lag + max T(p-1, s-1 .. s+1); items grouped by T,
+    // chunks of one group interleaved item by item.
+    const int P = 2 * ns;
+    std::vector<int> T((size_t)P * n);
+    for (int sl = 0; sl < n; ++sl) T[sl] = sl;
+    for (int ph = 1; ph < P; ++ph)
+      for (int sl = 0; sl < n; ++sl) {
+        int t = 0;
+        for (int d = -1; d <= 1; ++d) t = std::max(t, T[(size_t)(ph - 1) * n + (sl + d + n) % n]);
+        T[(size_t)ph * n + sl] = t + lag;
+      }
+    std::vector<int> items((size_t)P * n);
+    for (int i = 0; i < P * n; ++i) items[i] = i;
+    std::stable_sort(items.begin(), items.end(), [&](int x, int y) { return T[x] < T[y]; });
+    std::vector<int> sched;
+    sched.reserve((size_t)P * n * pl.cpi);
+    for (size_t a = 0; a < items.size();) {
+      size_t b = a;
+      while (b < items.size() && T[items[b]] == T[items[a]]) ++b;
+      for (int c = 0; c < pl.cpi; ++c)
+        for (size_t q = a; q < b; ++q) sched.push_back(items[q] * pl.cpi + c);
+      a = b;
+    }
+    pl.total[ns - 1] = (int)sched.size();
+    if ((e = cudaMalloc((void **)&pl.sched[ns - 1], sched.size() * sizeof(int))) != cudaSuccess) return e;
+    if ((e = cudaMemcpy(pl.sched[ns - 1], sched.data(), sched.size() * sizeof(int), cudaMemcpyHostToDevice)) !=
+        cudaSuccess)
+      return e;
+  }
+  const size_t nsync = kSyncDone + (size_t)2 * kHbMaxSweeps * n;
+  if ((e = cudaMalloc((void **)&pl.sync, nsync * sizeof(unsigned long long))) != cudaSuccess) return e;
+  if ((e = cudaMemset(pl.sync, 0, nsync * sizeof(unsigned long long))) != cudaSuccess) return e;
+  int dev = 0, sms = 0, occ = 0;
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, hb_ordered_kernel<false, false>, kHbOrderedThreads,
+                                                          0)) != cudaSuccess)
+    return e;
+  pl.grid = std::max(1, sms * std::max(1, occ));
+  return cudaSuccess;
+}
+
+void hb_plan_free(HbPlan &pl) {
+  for (int i = 0; i < kHbMaxSweeps; ++i) {
+    if (pl.sched[i]) cudaFree(pl.sched[i]);
+    pl.sched[i] = nullptr;
+    pl.total[i] = 0;
+  }
+  if (pl.sync) cudaFree(pl.sync);
+  pl.sync = nullptr;
+  pl.N = 0;
+}
+
+cudaError_t launch_hb_ordered(Fields f, int N, const HbArgs &a, const HbPlan &pl, int nsweeps, const uint64_t *sk,
+                              cudaStream_t st) {
+  if (pl.N != N || nsweeps < 1 || nsweeps > kHbMaxSweeps) return cudaErrorInvalidValue;
+  const bool inj = a.prop != nullptr, mon = a.mon != nullptr;
+  if ((inj || a.flags) && nsweeps != 1) return cudaErrorInvalidValue;
+  HbSched s{};
+  s.sched = pl.sched[nsweeps - 1];
+  s.sync = pl.sync;
+  s.total = pl.total[nsweeps - 1];
+  s.cpi = pl.cpi;
+  s.spc = pl.spc;
+  s.nslab = pl.nslab;
+  s.S = pl.S;
+  s.nphase = 2 * nsweeps;
+  s.limit = pl.wait_limit;
+  for (int q = 0; q < nsweeps; ++q) s.sk[q] = sk ? sk[q] : a.sk;
+  const Geo g = make_geo(N);
+  const int grid = std::min(pl.grid, s.total);
+  if (inj) {
+    if (mon) hb_ordered_kernel<true, true><<<grid, kHbOrderedThreads, 0, st>>>(f, g, a, s);
+    else hb_ordered_kernel<true, false><<<grid, kHbOrderedThreads, 0, st>>>(f, g, a, s);
+  } else {
+    if (mon) hb_ordered_kernel<false, true><<<grid, kHbOrderedThreads, 0, st>>>(f, g, a, s);
+    else hb_ordered_kernel<false, false><<<grid, kHbOrderedThreads, 0, st>>>(f, g, a, s);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t hb_plan_timeouts(const HbPlan &pl, cudaStream_t st, unsigned long long *out, bool clear) {
+  *out = 0;
+  if (!pl.sync) return cudaSuccess;
+  cudaError_t e = cudaMemcpyAsync(out, pl.sync + kSyncTimeouts, sizeof(*out), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess && clear && *out) e = cudaMemsetAsync(pl.sync + kSyncTimeouts, 0, sizeof(*out), st);
+  return e;
 }
 
 static int hb_zchunk(int N) {
