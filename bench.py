@@ -15,10 +15,12 @@ One process per GPU; for N > 1 each rank advances its own replica (distinct
 seed): the stepper does not shard, so scaling is weak, with no data-path
 collective.  Rank 0 prints one JSON line.
 
---impl reference times the reference algorithm on the host cores: the CPU
-restatement in oracle/ (the reference itself needs PETSc/MPI/HDF5/FFTW, absent
-here), drawing from the reference's own serial xoroshiro128+ stream, with one
-thread per emulated MPI rank on a bounded lattice sample.
+--impl reference times the reference's own implementation on the host cores:
+Stepper.cxx, NoiseGenerator.cxx and measurer.cxx compiled unmodified against
+single-node PETSc/MPI/FFTW stand-ins (oracle/_ref/ref_stepper, built with the
+oracle), one process per MPI rank, on the same 256^3 workload (K timed steps
+after W warm-up, measuring every 10).  Without that build it falls back to the
+oracle's restatement on a 128^3 sample.
 """
 import argparse
 import json
@@ -121,10 +123,45 @@ class ClockSampler:
                 "samples": len(mhz)}
 
 
-def cpu_reference_rate(N, scounts, seconds=15.0, steps=None, warmup=1):
-    """The reference algorithm on the host cores (oracle port, reference RNG)."""
+def reference_build_run(N, scounts, warmup, steps, ranks, seed=122335456):
+    """The reference's own stepper and measurer (oracle/_ref/ref_stepper: Stepper.cxx,
+    NoiseGenerator.cxx, measurer.cxx compiled unmodified against single-node
+    PETSc/MPI/FFTW stand-ins), one process per MPI rank (z-slabs), the
+    workload of run_ours: phi ~ 0.1 N(0,1) and Gaussian charges from the
+    reference's own stream, `warmup` untimed steps, then `steps` timed steps
+    with Measurer::measure every MEASURE_EVERY steps, as run_event does
+    (SuperPions.cxx:127-158).  Returns (site-updates/s, ms per step, seconds)."""
     sys.path.insert(0, os.path.join(REPO, "oracle"))
-    import numpy as np
+    import refbuild
+
+    name = "PV2HBSplit%d%d" % scounts
+    P = refbuild.params_json(N, mass0=COEF["mass0"], lam=COEF["lam"], H=COEF["H"], chi=COEF["chi"],
+                             gamma=COEF["gamma"], diffusion=COEF["diffusion"], seed=seed, dt=DT)
+    ops = ["phi=0.1", "charges"]
+    if warmup:
+        ops.append(f"step={name},{warmup}")
+    timed = []
+    s = 0
+    while s < steps:
+        n = min(MEASURE_EVERY, steps - s)
+        timed += ["measure", f"step={name},{n}"]
+        s += n
+    res = refbuild.run(P, ops + timed, ranks=ranks, timeout=3600)
+    el = sum(t for _, t in res.times[len(ops):])
+    return N ** 3 * steps / el, el / steps * 1e3, el
+
+
+def reference_available():
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import refbuild
+
+    return refbuild.available()
+
+
+def cpu_port_rate(N, scounts, steps, warmup=1):
+    """Fallback when the reference build is absent: the oracle's restatement
+    with the reference's serial RNG, one thread per emulated MPI rank."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
     import oracle
 
     cores = os.cpu_count() or 1
@@ -134,14 +171,30 @@ def cpu_reference_rate(N, scounts, seconds=15.0, steps=None, warmup=1):
     o.initialize(2)
     for _ in range(warmup):
         o.step(0, DT, inner=scounts[0], outer=scounts[1])
-    done, t0 = 0, time.perf_counter()
-    while True:
+    t0 = time.perf_counter()
+    for _ in range(steps):
         o.step(0, DT, inner=scounts[0], outer=scounts[1])
-        done += 1
-        el = time.perf_counter() - t0
-        if (steps is not None and done >= steps) or (steps is None and el >= seconds):
-            break
-    return N ** 3 * done / el, R, done, el
+    el = time.perf_counter() - t0
+    return N ** 3 * steps / el, el / steps * 1e3, el, R
+
+
+def cpu_baseline_sample(N, scounts):
+    """cpu_baseline of the GPU arm: a bounded sample (2 timed steps after 1
+    warm-up) of the same workload on all host cores."""
+    name = "PV2HBSplit%d%d" % scounts
+    cores = os.cpu_count() or 1
+    if reference_available():
+        R = max(1, min(cores, N // 2))
+        rate, ms, el = reference_build_run(N, scounts, 1, 2, R)
+        return {"value": rate, "unit": "site-updates/s", "cores": R, "kind": "reference",
+                "sample": f"2 timed {name} steps (after 1 warm-up, measurement every {MEASURE_EVERY}) of the {N}^3 "
+                          f"lattice, {el:.1f} s: the reference's Stepper.cxx/measurer.cxx built against single-node "
+                          f"PETSc/MPI stand-ins, {R} MPI ranks (processes, z-slabs)"}
+    Ns = min(N, 128)
+    rate, ms, el, R = cpu_port_rate(Ns, scounts, 2)
+    return {"value": rate, "unit": "site-updates/s", "cores": R, "kind": "port",
+            "sample": f"2 {name} steps of a {Ns}^3 sample lattice ({el:.1f} s), oracle port with the reference "
+                      f"serial RNG, one thread per emulated MPI rank"}
 
 
 def run_reference(a):
@@ -151,17 +204,29 @@ def run_reference(a):
     scounts = tuple(int(x) for x in a.scounts.split(","))
     name = "PV2HBSplit%d%d" % scounts
     cores = os.cpu_count() or 1
-    Ns = 128 if cores >= 16 else 64
-    rate, R, done, el = cpu_reference_rate(Ns, scounts, steps=a.steps, warmup=a.warmup)
-    sample = (f"{done} timed steps (+{a.warmup} warm-up) of {name} on a {Ns}^3 sample lattice of the "
-              f"{a.N}^3 workload, {R} threads = emulated MPI z-slab ranks, reference serial RNG")
+    config = {"workload": f"Model G {name}, {a.N}^3 periodic lattice, FP64, measure every {MEASURE_EVERY} steps",
+              "N": a.N, "evolver": name, "dt": DT, **COEF}
+    if reference_available():
+        R = max(1, min(cores, a.N // 2))
+        rate, ms, el = reference_build_run(a.N, scounts, a.warmup, a.steps, R)
+        cpu = {"kind": "reference", "cores": R,
+               "sample": f"the whole workload: {a.steps} timed steps after {a.warmup} warm-up on the {a.N}^3 "
+                         f"lattice ({el:.1f} s), the reference's Stepper.cxx/NoiseGenerator.cxx/measurer.cxx built "
+                         f"unmodified against single-node PETSc/MPI/FFTW stand-ins, {R} MPI ranks (processes)"}
+        config["implementation"] = "reference stepper and measurer (oracle/_ref/ref_stepper)"
+    else:
+        Ns = min(a.N, 128)
+        rate, ms, el, R = cpu_port_rate(Ns, scounts, a.steps, a.warmup)
+        cpu = {"kind": "port", "cores": R,
+               "sample": f"{a.steps} timed steps of a {Ns}^3 sample lattice ({el:.1f} s), oracle port with the "
+                         f"reference serial RNG; the reference build is absent"}
+        config["sample_N"] = Ns
+    cpu.update(value=rate, unit="site-updates/s")
     line = {
         "impl": "reference", "metric": "Model G site-updates/s", "value": rate, "unit": "site-updates/s",
-        "n_gpus": a.gpus, "steps": done, "warmup": a.warmup, "ms_per_step": el / done * 1e3 * (a.N / Ns) ** 3,
+        "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"Model G {name}, {a.N}^3 periodic, FP64 (CPU on a {Ns}^3 sample)", "N": a.N,
-                   "sample_N": Ns, "dt": DT, **COEF},
-        "cpu_baseline": {"value": rate, "unit": "site-updates/s", "cores": R, "kind": "port", "sample": sample},
+        "config": config, "cpu_baseline": cpu,
         "e2e": {"value": rate, "unit": "site-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -619,8 +684,7 @@ def run_ours(a):
         one_step(s)
     torch.cuda.synchronize()
 
-    # ---- timed region: device-resident state ---------------------------------
-    L.check(lib.lgv_timing_enable(h, 1), "timing")
+    # ---- timed region: device-resident state, no per-launch instrumentation ---
     clocks = ClockSampler(local)
     time.sleep(0.3)
     if dist:
@@ -636,16 +700,24 @@ def run_ours(a):
         dist.barrier()
     ck = clocks.stop()
     ms = max_over_ranks(e0.elapsed_time(e1), dist, "cuda")
+    n_meas = len(range(0, a.steps, MEASURE_EVERY))
+
+    # ---- per-kernel split: the same steps again with an event pair around every launch
+    split_steps = min(a.steps, 20)
+    L.check(lib.lgv_timing_enable(h, 1), "timing")
+    for s in range(split_steps):
+        one_step(s)
+    torch.cuda.synchronize()
     kern = {}
     for k, c in KCLASS.items():
         tot, n = C.c_double(), C.c_int64()
         L.check(lib.lgv_timing_read(h, c, C.byref(tot), C.byref(n)), "timing_read")
         kern[k] = (tot.value, n.value)
     L.check(lib.lgv_timing_enable(h, 0), "timing off")
-    n_meas = len(range(0, a.steps, MEASURE_EVERY))
-    launches = 0
-    for k, (tot, n) in kern.items():
-        launches += n * (5 if k == "measure" else 1)
+    # launches of the timed region: the split pass's count per step (the
+    # measurement every MEASURE_EVERY steps is 5 launches)
+    per_step = sum(n for k, (tot, n) in kern.items() if k != "measure") / split_steps
+    launches = int(round(per_step * a.steps)) + 5 * n_meas
 
     value = whole_job_rate(V * a.steps, world, ms / 1e3)
     peak, peak_kind = peaks()
@@ -654,19 +726,24 @@ def run_ours(a):
     avg_ms = tot / n
     alg = ALG_BYTES[dom] * V
     achieved = alg / (avg_ms / 1e3) / 1e9
-    trow = traffic_table().get(dom)
+    ttab = traffic_table()
+    trow = ttab.get(dom)
     traffic = None
     if trow:
+        # measured per site at 256^3 (profiles/traffic.json), per launch of this lattice
         traffic = trow["bytes_per_site"] * V
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
                 if peak_kind == "measured" else "fallback 6.65 TB/s",
                 "traffic": traffic, "alg_bytes_per_launch": alg, "avg_launch_ms": avg_ms,
+                "traffic_over_alg": (traffic / alg) if traffic else None,
                 "frac_of_nominal": achieved / NOMINAL_HBM_GBS, "nominal_GBps": NOMINAL_HBM_GBS}
     kernels = {k: {"launches": kern[k][1], "total_ms": kern[k][0],
                    "avg_ms": (kern[k][0] / kern[k][1]) if kern[k][1] else None,
                    "alg_GBps": (ALG_BYTES[k] * V / (kern[k][0] / kern[k][1] / 1e3) / 1e9)
-                   if (k in ALG_BYTES and kern[k][1]) else None}
+                   if (k in ALG_BYTES and kern[k][1]) else None,
+                   "traffic_over_alg": (ttab[k]["bytes_per_site"] / ttab[k]["alg_bytes_per_site"])
+                   if k in ttab else None}
                for k in kern}
     step_frac = STEP_BYTES.get(name, float("nan")) * V * a.steps * 1.0 / (ms / 1e3) / 1e9 / peak
 
@@ -699,11 +776,7 @@ def run_ours(a):
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        rate, R, done, el = cpu_reference_rate(128 if (os.cpu_count() or 1) >= 16 else 64, scounts, seconds=12.0)
-        Ns = 128 if (os.cpu_count() or 1) >= 16 else 64
-        cpu = {"value": rate, "unit": "site-updates/s", "cores": R, "kind": "port",
-               "sample": f"{done} {name} steps on a {Ns}^3 sample lattice ({el:.1f} s), oracle port with the "
-                         f"reference serial RNG, one thread per emulated MPI rank"}
+        cpu = cpu_baseline_sample(N, scounts)
 
     # ---- the other steppers on the same 256^3 lattice ---------------------------
     variants = None
@@ -768,6 +841,19 @@ def run_ours(a):
         "gpu_launches": launches,
         "clocks": ck,
     }
+    # The targets in a few compact keys at the end of the line (a truncated
+    # log tail still shows them).
+    summary = {"step_hbm_frac": step_frac, "ms_per_step": ms / a.steps,
+               "dominant_kernel": dom, "dominant_kernel_frac": roofline["frac"]}
+    if ensemble:
+        summary["ensemble_speedup_vs_plain"] = ensemble["speedup_vs_plain"]
+    if adjoint:
+        summary["adjoint_over_forward"] = adjoint.get("adjoint_over_forward")
+        if adjoint.get("batched"):
+            summary["batched_adjoint_over_forward"] = adjoint["batched"].get("adjoint_over_forward")
+    if cpu:
+        summary["gpu_over_cpu_baseline"] = value / cpu["value"]
+    line["summary"] = summary
     print(json.dumps(line))
     return 0
 

@@ -294,7 +294,7 @@ class ModelAData {
 
 // ---------------------------------------------------------------------------
 // NoiseGenerator (NoiseGenerator.h:62-157): the reference's serial host stream.
-class xoroshiro128plus {  // xoroshiro128plus.h:227-313
+class xoroshiro128plus {  // xoroshiro128plus.h:63-149 (engine :86-107, stream I/O :137-142)
  public:
   typedef uint64_t result_type;
   static constexpr uint64_t min() { return 0; }

@@ -42,11 +42,20 @@ __host__ __device__ __forceinline__ long long rb_off(const Geo &g, int i, int j,
 __device__ __forceinline__ int wrap_inc(int a, int n) { return (a + 1 == n) ? 0 : a + 1; }
 __device__ __forceinline__ int wrap_dec(int a, int n) { return (a == 0) ? n - 1 : a - 1; }
 
-// Counter-indexed xoroshiro128+ streams -------------------------------------
-// A stream is identified by (sub-step key sk, index n); its 128-bit state is
-// splitmix64 outputs 2n and 2n+1 of the sequence seeded with sk.  The engine
-// is the reference's xoroshiro128+ (rotations 55/14/36,
-// xoroshiro128plus.h:261-271).
+// Counter-indexed noise ------------------------------------------------------
+// Every sub-step has a key sk; word w of it is splitmix64 output w of the
+// sequence seeded with sk (split_word).  Stream n is a xoroshiro128+
+// generator -- the reference's engine, rotations 55/14/36,
+// xoroshiro128plus.h:86-107 -- whose 128-bit state is words 2n and 2n+1: the
+// heat-bath site n draws its four proposals and then, only when dS >= 0, its
+// accept uniform from it (53-bit uniforms), and the Gaussian draws
+// (Euler-Maruyama, initial states) come from it.  The charge link of A-site n
+// takes 32-bit uniforms straight from words 6n .. 6n+5 instead (component L:
+// the proposal from the low half of word 6n+L, the accept uniform from its
+// high half): six splitmix64 outputs per link cost fewer instructions than a
+// stream's two seeding outputs and twelve steps, and measured faster, while
+// for the heat bath the stream measured faster (0.180 against 0.196 ms per
+// 256^3 pass on one B200).
 static constexpr uint64_t kGolden = 0x9E3779B97F4A7C15ull;
 
 __host__ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
@@ -80,6 +89,26 @@ __device__ __forceinline__ Xoro stream_at(uint64_t sk, uint64_t n) {
   x.s0 = split_word(sk, 2 * n);
   x.s1 = split_word(sk, 2 * n + 1);
   return x;
+}
+
+// Consecutive words w0, w0 + 1, ... of the sequence of sub-step key sk.
+struct WordStream {
+  uint64_t z;  // sk + (w + 1) * kGolden for the next word w
+  __device__ __forceinline__ uint64_t next() {
+    const uint64_t r = mix64(z);
+    z += kGolden;
+    return r;
+  }
+};
+__device__ __forceinline__ WordStream words_at(uint64_t sk, uint64_t w0) { return WordStream{sk + (w0 + 1) * kGolden}; }
+__device__ __forceinline__ uint32_t lo32(uint64_t r) { return (uint32_t)r; }
+__device__ __forceinline__ uint32_t hi32(uint64_t r) { return (uint32_t)(r >> 32); }
+// uniform in (0,1) from 32 bits: (k + 1/2) 2^-32, exact and symmetric about 1/2
+__device__ __forceinline__ double u32(uint32_t k) { return fma((double)k, 0x1p-32, 0x1p-33); }
+// variance-1 uniform in (-sqrt3, sqrt3) from 32 bits: ((k + 1/2) 2^-31 - 1) sqrt3;
+// the bracket is exact, the product rounds once
+__device__ __forceinline__ double v32(uint32_t k) {
+  return __dmul_rn(fma((double)k, 0x1p-31, 0x1p-32 - 1.0), 1.7320508075688772);
 }
 
 // uniform in [0,1) from the top 53 bits (exact conversion)

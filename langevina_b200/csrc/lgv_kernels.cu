@@ -388,6 +388,114 @@ __global__ void __launch_bounds__(128) hb_pass_kernel(Fields f, Geo g, int parit
 }
 
 // ----------------------------------------------------------------------------
+// Phi heat bath, one checkerboard parity per launch, z-marching
+// (EulerLangevinHB::step, Stepper.cxx:325-381).  A CTA of 32 x ZP_TY threads
+// owns elements m0 .. m0+31 of half rows j0 .. j0+ZP_TY-1 and marches up a
+// z-chunk.  The other parity's values of each plane are loaded once: the
+// thread's own element stays in registers for three planes (its z-1, z and
+// z+1 neighbours), and the plane's tile with a one-element ring goes to
+// shared memory for the x and y neighbours.  A site therefore costs 8 global
+// loads (its own 4 components and the other parity's 4 of the plane above)
+// plus the ring's share, against 28 for hb_pass_kernel, and every value of
+// the other parity crosses L2 about once.  Decisions, streams and results are
+// those of hb_site.
+constexpr int ZP_TM = 32, ZP_TY = 8, ZP_NT = ZP_TM * ZP_TY;
+constexpr int ZP_W = ZP_TM + 2, ZP_R = ZP_TY + 2, ZP_PL = ZP_W * ZP_R;  // padded tile of one component
+constexpr int ZP_RING = 2 * ZP_TM + 2 * ZP_TY;
+
+template <bool INJECTED, bool MON>
+__global__ void __launch_bounds__(ZP_NT) hb_zpass_kernel(Fields f, Geo g, int parity, int zchunk, HbArgs a) {
+  __shared__ double tile[2][4][ZP_PL];
+  const int N = g.N, H = g.H;
+  const int tm = threadIdx.x, ty = threadIdx.y, tid = ty * ZP_TM + tm;
+  const int m0 = blockIdx.x * ZP_TM, j0 = blockIdx.y * ZP_TY;
+  const int k0 = blockIdx.z * zchunk, k1 = min(k0 + zchunk, N);
+  const int tme = min(ZP_TM, H - m0), tye = min(ZP_TY, N - j0);  // valid extent of this tile
+  const bool own = tm < tme && ty < tye;
+  const int m = m0 + tm, j = j0 + ty;
+  const long long ob = (long long)(parity ^ 1) * g.V2, pb = (long long)parity * g.V2;
+  // ring element of this thread (tid < ZP_RING): padded position (rx, ry) and half-row element (rm, rj)
+  // rows above and below the tile (tme elements each), then the columns left
+  // and right of it (tye rows each); corners are not needed
+  int rx = 0, ry = 0, rm = 0, rj = 0;
+  bool ring_live = false;
+  if (tid < ZP_TM) {
+    rx = 1 + tid, ry = 0, ring_live = tid < tme;
+  } else if (tid < 2 * ZP_TM) {
+    rx = 1 + tid - ZP_TM, ry = tye + 1, ring_live = tid - ZP_TM < tme;
+  } else if (tid < 2 * ZP_TM + ZP_TY) {
+    rx = 0, ry = 1 + tid - 2 * ZP_TM, ring_live = tid - 2 * ZP_TM < tye;
+  } else if (tid < ZP_RING) {
+    rx = tme + 1, ry = 1 + tid - 2 * ZP_TM - ZP_TY, ring_live = tid - 2 * ZP_TM - ZP_TY < tye;
+  }
+  if (ring_live) {
+    rm = m0 + rx - 1;
+    rj = j0 + ry - 1;
+    rm = rm < 0 ? rm + H : (rm >= H ? rm - H : rm);
+    rj = rj < 0 ? rj + N : (rj >= N ? rj - N : rj);
+  }
+  // the other parity's values of plane kk: own element -> o[], ring element -> smem
+  auto load_other = [&](int kk, double (&o)[4], int buf) {
+    const int kw = kk < 0 ? kk + N : (kk >= N ? kk - N : kk);
+    if (own) {
+      const long long off = ob + ((long long)kw * N + j) * H + m;
+#pragma unroll
+      for (int l = 0; l < 4; ++l) o[l] = f.c[l][off];
+    }
+    if (ring_live) {
+      const long long off = ob + ((long long)kw * N + rj) * H + rm;
+#pragma unroll
+      for (int l = 0; l < 4; ++l) tile[buf][l][ry * ZP_W + rx] = f.c[l][off];
+    }
+  };
+  double oz[4] = {0, 0, 0, 0}, oc[4] = {0, 0, 0, 0}, on[4] = {0, 0, 0, 0};
+  load_other(k0 - 1, oz, 0);  // only the own element is used (z-1 neighbour); the ring is overwritten below
+  load_other(k0, oc, 0);
+  if (own) {
+#pragma unroll
+    for (int l = 0; l < 4; ++l) tile[0][l][(ty + 1) * ZP_W + tm + 1] = oc[l];
+  }
+  __syncthreads();
+  MonLocal mon;
+  for (int k = k0; k < k1; ++k) {
+    const int b = (k - k0) & 1;
+    load_other(k + 1, on, b ^ 1);
+    if (own) {
+      const int s = (parity + j + k) & 1;
+      const double *T = &tile[b][0][0];
+      const int c = (ty + 1) * ZP_W + tm + 1;
+      const long long offp = pb + ((long long)k * N + j) * H + m;
+      double po[4], heff[4];
+#pragma unroll
+      for (int l = 0; l < 4; ++l) {
+        const double *Tl = T + l * ZP_PL;
+        // x neighbours: elements m-1+s and m+s of the other parity's row
+        heff[l] = (Tl[c + s] + Tl[c - 1 + s]) + (Tl[c + ZP_W] + Tl[c - ZP_W]) + (on[l] + oz[l]);
+        po[l] = f.c[l][offp];
+      }
+      const long long nat = ((long long)k * N + j) * N + 2 * m + s;
+      HbDecision d;
+      hb_decide<INJECTED>(po, heff, a, nat, 2 * g.V2, d);
+      if (d.accept) {
+#pragma unroll
+        for (int l = 0; l < 4; ++l) f.c[l][offp] = d.pn[l];
+      }
+      if (MON) mon_count(mon, d);
+      if (a.flags) a.flags[nat] = d.flag;
+#pragma unroll
+      for (int l = 0; l < 4; ++l) tile[b ^ 1][l][c] = on[l];
+    }
+#pragma unroll
+    for (int l = 0; l < 4; ++l) {
+      oz[l] = oc[l];
+      oc[l] = on[l];
+    }
+    __syncthreads();
+  }
+  if (MON) mon_flush(mon, a.mon);
+}
+
+// ----------------------------------------------------------------------------
 // Phi heat bath, one or more whole sweeps (EulerLangevinHB::step,
 // Stepper.cxx:287-389) in one persistent launch, ordered through the lattice
 // by z-slabs so that the odd pass of a slab runs while its phi is still in
@@ -683,8 +791,8 @@ __device__ __forceinline__ void charge_link_site(const Fields &f, const Geo &g, 
   }
   const long long nat = ((long long)k * N + j) * N + i;
   const long long V = 2 * g.V2;
-  Xoro rng;
-  if (!INJECTED) rng = stream_at(a.sk, (uint64_t)nat);
+  WordStream ws{};
+  if (!INJECTED) ws = words_at(a.sk, 6 * (uint64_t)nat);
 #pragma unroll
   for (int L = 0; L < 6; ++L) {
     double *P = f.c[4 + L];
@@ -695,8 +803,8 @@ __device__ __forceinline__ void charge_link_site(const Fields &f, const Geo &g, 
     if (INJECTED) {
       v = a.q[ii];
     } else {
-      v = var1(rng.next());
-      ra = rng.next();
+      ra = ws.next();
+      v = v32(lo32(ra));
     }
     const double q = a.rms * v;
     const double dA = nA - q, dB = nB + q;
@@ -708,7 +816,7 @@ __device__ __forceinline__ void charge_link_site(const Fields &f, const Geo &g, 
       fl = 1;
       if (MON) mon.down(dS);
     } else {
-      const double r = INJECTED ? a.acc[ii] : u53(ra);
+      const double r = INJECTED ? a.acc[ii] : u32(hi32(ra));
       accept = r < exp(-dS);
       fl = accept ? 2 : 0;
       if (MON) {
@@ -754,8 +862,8 @@ struct ChargeDirArgs {
 template <bool INJECTED, bool MON>
 __device__ __forceinline__ void charge_link(double nA[6], double nB[6], const ChargeDirArgs &a, int pi,
                                             long long natA, long long V, bool own, MonLocal &mon) {
-  Xoro rng;
-  if (!INJECTED) rng = stream_at(a.sk[pi], (uint64_t)natA);
+  WordStream ws{};
+  if (!INJECTED) ws = words_at(a.sk[pi], 6 * (uint64_t)natA);
 #pragma unroll
   for (int L = 0; L < 6; ++L) {
     const long long ii = (long long)(a.pass[pi] * 6 + L) * V + natA;
@@ -764,8 +872,8 @@ __device__ __forceinline__ void charge_link(double nA[6], double nB[6], const Ch
     if (INJECTED) {
       v = a.q[ii];
     } else {
-      v = var1(rng.next());
-      ra = rng.next();
+      ra = ws.next();
+      v = v32(lo32(ra));
     }
     const double q = a.rms * v;
     const double dA = nA[L] - q, dB = nB[L] + q;
@@ -776,7 +884,7 @@ __device__ __forceinline__ void charge_link(double nA[6], double nB[6], const Ch
       accept = true;
       fl = 1;
     } else {
-      const double r = INJECTED ? a.acc[ii] : u53(ra);
+      const double r = INJECTED ? a.acc[ii] : u32(hi32(ra));
       accept = r < exp(-dS);
       fl = accept ? 2 : 0;
     }
@@ -2229,7 +2337,39 @@ static cudaError_t allow_smem(K kernel, size_t bytes) {
   return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
+// The z-marching pass is opt-in (LGV_HB_ZPASS=1 in the environment, for half
+// rows of at least one tile): on B200 at 256^3 it measured 0.22 ms per pass
+// against 0.19 ms for hb_pass_kernel -- at 80 registers three CTAs of 8 warps
+// per SM wait out the load of the plane above on every plane.
+static bool hb_zpass_default(int N) {
+  static const bool on = [] {
+    const char *v = std::getenv("LGV_HB_ZPASS");
+    return v && v[0] == '1';
+  }();
+  return on && N / 2 >= ZP_TM;
+}
+
+cudaError_t launch_hb_zpass(Fields f, int N, int parity, const HbArgs &a, cudaStream_t st) {
+  const Geo g = make_geo(N);
+  const long long bxy = (long long)((g.H + ZP_TM - 1) / ZP_TM) * ((N + ZP_TY - 1) / ZP_TY);
+  long long zc = (long long)N * bxy / (148 * 4 * 3);  // about three waves of 4 CTAs per SM
+  zc = std::max(4LL, std::min(32LL, zc));
+  zc = std::min<long long>(zc, N);
+  const dim3 grid((g.H + ZP_TM - 1) / ZP_TM, (N + ZP_TY - 1) / ZP_TY, (unsigned)((N + zc - 1) / zc));
+  const dim3 block(ZP_TM, ZP_TY);
+  const bool inj = a.prop != nullptr, mon = a.mon != nullptr;
+  if (inj) {
+    if (mon) hb_zpass_kernel<true, true><<<grid, block, 0, st>>>(f, g, parity, (int)zc, a);
+    else hb_zpass_kernel<true, false><<<grid, block, 0, st>>>(f, g, parity, (int)zc, a);
+  } else {
+    if (mon) hb_zpass_kernel<false, true><<<grid, block, 0, st>>>(f, g, parity, (int)zc, a);
+    else hb_zpass_kernel<false, false><<<grid, block, 0, st>>>(f, g, parity, (int)zc, a);
+  }
+  return cudaGetLastError();
+}
+
 cudaError_t launch_hb_pass(Fields f, int N, int parity, const HbArgs &a, cudaStream_t st) {
+  if (hb_zpass_default(N)) return launch_hb_zpass(f, N, parity, a, st);
   const Geo g = make_geo(N);
   const bool rows = g.H % 128 == 0;
   const dim3 grid = pass_grid(g, rows);

@@ -42,7 +42,7 @@
 namespace orc {
 
 // ---------------------------------------------------------------------------
-// xoroshiro128+ with the reference's seeding (xoroshiro128plus.h:250-271).
+// xoroshiro128+ with the reference's seeding (xoroshiro128plus.h:86-107).
 struct Xoro {
   using result_type = uint64_t;
   uint64_t s[2] = {0, 0};
@@ -91,6 +91,11 @@ struct NoiseGen {
 //   stream n   : xoroshiro128+ state (word(sk, 2n), word(sk, 2n + 1))
 //   uniform    : (r >> 11) * 2^-53 in [0, 1)
 //   variance1  : (2u - 1) * sqrt(3)
+//   phi heat bath, site n: stream n -> 4 proposals, then the accept uniform
+//     only if dS >= 0;  Gaussian draws: stream n
+//   charge link, A-site n, component L: 32-bit uniforms from word 6n+L,
+//     u32(k) = (k + 1/2) 2^-32, v32(k) = ((k + 1/2) 2^-31 - 1) sqrt(3):
+//     the proposal from the low half, the accept uniform from the high half
 static constexpr uint64_t G = 0x9E3779B97F4A7C15ull;
 static inline uint64_t mix(uint64_t z) {
   z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
@@ -103,6 +108,10 @@ static inline uint64_t word(uint64_t sk, uint64_t w) { return mix(sk + (w + 1) *
 static const double SQRT3 = std::sqrt(3.0);
 static inline double u53(uint64_t r) { return (double)(r >> 11) * 0x1p-53; }
 static inline double v1_of(uint64_t r) { return (2.0 * u53(r) - 1.0) * SQRT3; }
+static inline double u32_of(uint32_t k) { return ((double)k + 0.5) * 0x1p-32; }
+static inline double v32_of(uint32_t k) { return (((double)k + 0.5) * 0x1p-31 - 1.0) * SQRT3; }
+static inline uint32_t lo32(uint64_t r) { return (uint32_t)r; }
+static inline uint32_t hi32(uint64_t r) { return (uint32_t)(r >> 32); }
 struct CtrStream {
   Xoro x;
   CtrStream(uint64_t sk, uint64_t n) {
@@ -452,14 +461,13 @@ static void charge_hb(Handle &h, double dt) {
             for (int i = 0; i < h.N; ++i) {
               if ((k + j + i) % 2 != eoA) continue;
               const size_t nA = h.idx(i, j, k), nB = h.idx(i + di, j + dj, k + dk);
-              CtrStream cs(sk, h.mode == CTR ? nA : 0);
               for (int L = 4; L < 10; ++L) {
                 const double a = S[nA * LGV_NDOF + L], b = S[nB * LGV_NDOF + L];
                 const size_t ii = ((size_t)(pass * 6 + (L - 4))) * h.V + nA;
-                uint64_t rq = 0, ra = 0;
+                uint64_t ra = 0;
                 double v;
                 if (h.mode == SEQ) v = g.variance1();
-                else if (h.mode == CTR) { rq = cs.next(); ra = cs.next(); v = v1_of(rq); }
+                else if (h.mode == CTR) { ra = word(sk, 6 * (uint64_t)nA + (L - 4)); v = v32_of(lo32(ra)); }
                 else v = h.ch_q[ii];
                 // modelg_update_charge_pair (:419-441)
                 double q = rms * v;
@@ -472,7 +480,7 @@ static void charge_hb(Handle &h, double dt) {
                 } else {
                   double rr;
                   if (h.mode == SEQ) rr = g.uniform();
-                  else if (h.mode == CTR) rr = u53(ra);
+                  else if (h.mode == CTR) rr = u32_of(hi32(ra));
                   else rr = h.ch_acc[ii];
                   if (rr < std::exp(-dS)) {
                     mon_up_yes(m, dS);

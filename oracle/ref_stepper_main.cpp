@@ -13,6 +13,8 @@
 // params.json is the reference's input file (ModelAData(Json::Value&),
 // ModelA.h:222-248).  Operations, in order:
 //   load=FILE             state from FILE: N^3 * 10 doubles, u[k][j][i][L]
+//   phi=SCALE             ModelA::initialize with phi_a = SCALE * normal() from
+//                         the reference's stream, charges 0 (ModelA.h:408-461)
 //   charges               ModelA::initialize_gaussian_charges (ModelA.h:463-525)
 //   step=NAME,n           n x { NAME.step(atime.dt()); atime += atime.dt() }
 //   sub=NAME,n,d          n x NAME.step(atime.dt() / d), clock unchanged (the
@@ -73,6 +75,12 @@ void append(std::vector<double> &v, const std::vector<std::complex<double>> &a) 
   }
 }
 
+// Initial condition for ModelA::initialize: phi_a ~ scale * N(0, 1) drawn
+// from the reference's global stream, charges zero.
+double gaussian_phi(const double &, const double &, const double &, const int &L, void *params) {
+  return L < ModelAData::Nphi ? *(const double *)params * ModelARndm->normal() : 0.0;
+}
+
 std::unique_ptr<Stepper> make_stepper(const std::string &name, ModelA &model) {
   if (name == "IdealPV2") return std::make_unique<IdealPV2>(model);
   if (name == "EulerLangevinHB") return std::make_unique<EulerLangevinHB>(model);
@@ -129,6 +137,9 @@ int run(const std::string &params_path, const std::string &out_path, const std::
       const size_t n = u->hi - u->lo;
       if (std::fread(u->a + u->lo, sizeof(double), n, f) != n) lgvshim::fail("short state file");
       std::fclose(f);
+    } else if (verb == "phi") {
+      double scale = std::stod(arg);
+      model.initialize(gaussian_phi, &scale);
     } else if (verb == "charges") {
       model.initialize_gaussian_charges();
     } else if (verb == "step" || verb == "sub") {

@@ -79,7 +79,7 @@ int main() {
     xoroshiro128plus g;
     g.seed(s);
     std::ostringstream os;
-    os << g;  // stream format of the .rng restart file (xoroshiro128plus.h:301-303)
+    os << g;  // stream format of the .rng restart file (xoroshiro128plus.h:137-142)
     printf("state %" PRIu64 " %s %d", s, os.str().c_str(), n);
     for (int i = 0; i < n; ++i) printf(" %" PRIu64, g());
     printf("\n");

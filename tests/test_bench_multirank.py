@@ -70,7 +70,8 @@ def test_reference_arm_runs_on_rank_zero_only(monkeypatch):
     monkeypatch.setenv("RANK", "1")
     monkeypatch.setenv("WORLD_SIZE", "2")
     called = []
-    monkeypatch.setattr(bench, "cpu_reference_rate", lambda *a, **k: called.append(1))
+    monkeypatch.setattr(bench, "reference_build_run", lambda *a, **k: called.append(1))
+    monkeypatch.setattr(bench, "cpu_port_rate", lambda *a, **k: called.append(1))
     args = type("A", (), dict(scounts="2,3", steps=2, warmup=1, N=256, gpus=2))()
     buf = io.StringIO()
     with contextlib.redirect_stdout(buf):
@@ -86,3 +87,25 @@ def test_single_process_defaults(monkeypatch):
     assert bench.rank_env() == (1, 0, 0)
     assert bench.max_over_ranks(3.5, None, "cpu") == 3.5
     assert bench.replica_seed(7, 0) == 7
+
+
+def test_reference_arm_line_on_rank_zero(monkeypatch):
+    """Rank 0 prints one reference line on the arm's metric and config, its
+    measured ms_per_step unscaled, with cpu_baseline and a zero-copy e2e."""
+    import json
+
+    import bench
+
+    for k in ("RANK", "WORLD_SIZE", "LOCAL_RANK"):
+        monkeypatch.delenv(k, raising=False)
+    monkeypatch.setattr(bench, "reference_available", lambda: True)
+    monkeypatch.setattr(bench, "reference_build_run", lambda N, sc, w, k, R: (1.0e6, 16.7e3, 16.7 * k))
+    args = type("A", (), dict(scounts="2,3", steps=3, warmup=1, N=256, gpus=1))()
+    buf = io.StringIO()
+    with contextlib.redirect_stdout(buf):
+        assert bench.run_reference(args) == 0
+    line = json.loads(buf.getvalue())
+    assert line["impl"] == "reference" and line["metric"] == "Model G site-updates/s"
+    assert line["ms_per_step"] == 16.7e3 and line["steps"] == 3 and line["config"]["N"] == 256
+    assert line["cpu_baseline"]["kind"] == "reference" and line["e2e"]["h2d_bytes_per_step"] == 0
+
