@@ -20,6 +20,8 @@
 //   sub=NAME,n,d          n x NAME.step(atime.dt() / d), clock unchanged (the
 //                         thermalisation loop, SuperPions.cxx:47-53)
 //   measure               Measurer::measure; appends the packed measurement
+//   sample=NAME,n,every   n x { every x NAME.step(atime.dt()); Measurer::measure },
+//                         appending OAverage (11 doubles) of each measurement
 //   save                  appends the state
 //   energy                appends IdealPV2::computeEnergy of the state
 //   finalize              finalize() of every stepper built so far (the
@@ -30,7 +32,7 @@
 // out.bin is a sequence of records {u32 tag, u64 count, count doubles}; tags:
 // 1 state, 2 measurement (OAverage, wall[3], wall_k[3], wall_k_rotated[3],
 // wall_phase[3], wall_phase_k[3], each row-major, complex as re, im), 3
-// energy.  Rank 0 writes it.  For every operation rank 0 prints
+// energy, 4 OAverage of a sample.  Rank 0 writes it.  For every operation rank 0 prints
 // "REFTIME <op> <seconds>" (wall clock between barriers), and at the end one
 // "REFEVENT <name> <seconds> <count>" line per PetscLogEvent of the stepper.
 //
@@ -166,6 +168,25 @@ int run(const std::string &params_path, const std::string &out_path, const std::
       } else {
         const double d = std::stod(f[2]);
         for (int s = 0; s < n; ++s) it->second->step(atime.dt() / d);
+      }
+    } else if (verb == "sample") {
+      const size_t c1 = arg.find(','), c2 = arg.find(',', c1 + 1);
+      if (c1 == std::string::npos || c2 == std::string::npos) lgvshim::fail("bad sample operation");
+      const std::string name = arg.substr(0, c1);
+      const int n = std::stoi(arg.substr(c1 + 1, c2 - c1 - 1)), every = std::stoi(arg.substr(c2 + 1));
+      auto it = steppers.find(name);
+      if (it == steppers.end()) {
+        it = steppers.emplace(name, make_stepper(name, model)).first;
+        built.push_back(name);
+      }
+      if (!measurer) measurer = std::make_unique<Measurer>(&model);
+      for (int c = 0; c < n; ++c) {
+        for (int s = 0; s < every; ++s) {
+          it->second->step(atime.dt());
+          atime += atime.dt();
+        }
+        measurer->measure(&model.solution);
+        if (rank == 0) out.rec(4, measurer->OAverage.data(), measurer->OAverage.size());
       }
     } else if (verb == "measure") {
       if (!measurer) measurer = std::make_unique<Measurer>(&model);

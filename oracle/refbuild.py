@@ -90,6 +90,7 @@ class Result:
         self.states = [v.reshape(N, N, N, 10) for t, v in records if t == 1]
         self.measurements = [unpack_measurement(N, v) for t, v in records if t == 2]
         self.energies = [float(v[0]) for t, v in records if t == 3]
+        self.averages = np.array([v for t, v in records if t == 4]).reshape(-1, NOBS)
         self.stdout = stdout
         self.times = [(m.group(1), float(m.group(2))) for m in re.finditer(r"^REFTIME (\S+) (\S+)$", stdout, re.M)]
         self.events = {m.group(1): (float(m.group(2)), int(m.group(3)))
