@@ -313,10 +313,13 @@ int lgv_ensemble_synchronize(lgv_ensemble *e);
  * is a static device array inside the library sized for N <= 128 (6.55 MB,
  * held on every GPU that loads the library until exit); larger N is rejected
  * with LGV_ERR_INVALID.  The array is shared by all calls on a device, so calls
- * whose kernels overlap on the GPU race with each other.  The first call on a
- * device looks the array up (cudaGetSymbolAddress) with that device current;
- * make that first call before any stream capture.  Asynchronous on `stream`
- * (NULL = legacy default stream); calls no allocator. */
+ * whose kernels overlap on the GPU race with each other.  A call made outside
+ * stream capture looks the array's address up (cudaGetSymbolAddress) in the
+ * current device's context; a call made while `stream` is being captured uses
+ * the address its device's last uncaptured call found, and fails with
+ * LGV_ERR_STATE if there was none -- so make the first call on each device
+ * before any stream capture.  Asynchronous on `stream` (NULL = legacy default
+ * stream); calls no allocator. */
 #define LGV_NOALLOC_MAX_N 128
 int lgv_measure_aos_noalloc(const double *dev_aos, int N, double *dev_out, void *stream);
 

@@ -18,9 +18,13 @@
 //    needs clearing between calls; but two calls whose kernels overlap on the
 //    GPU (different streams without ordering, or several host threads) race
 //    on the array and corrupt each other's results.
-//  - The array's device address is looked up once per device, by the first
-//    call made with that device current; make that first call before any
-//    stream capture begins.
+//  - Host code cannot use g_scratch's name as a device address: every call
+//    made outside stream capture looks the address up with
+//    cudaGetSymbolAddress for the current device (so a context made anew,
+//    e.g. after cudaDeviceReset, is followed) and records it; a call made
+//    while `stream` is being captured uses the address recorded for its
+//    device.  So make the first call on each device before any capture
+//    begins.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -57,21 +61,27 @@ extern "C" int lgv_measure_aos_noalloc(const double *dev_aos, int N, double *dev
   int dev = -1;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
     return fail(LGV_ERR_CUDA, "lgv_measure_aos_noalloc: no usable current CUDA device");
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cap) != cudaSuccess)
+    return fail(LGV_ERR_CUDA, "lgv_measure_aos_noalloc: cudaStreamIsCapturing failed");
   double *scratch = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_scratch_addr[dev]) {
-      // host code may not use g_scratch directly: resolve its address on this device
-      const cudaError_t e = cudaGetSymbolAddress((void **)&g_scratch_addr[dev], g_scratch);
-      if (e != cudaSuccess) {
-        g_scratch_addr[dev] = nullptr;
+    if (cap == cudaStreamCaptureStatusNone) {
+      // host code may not use g_scratch directly: resolve its address in the current context
+      double *p = nullptr;
+      if (cudaGetSymbolAddress((void **)&p, g_scratch) != cudaSuccess || !p)
         return fail(LGV_ERR_CUDA, "lgv_measure_aos_noalloc: cudaGetSymbolAddress of the static scratch failed");
-      }
+      g_scratch_addr[dev] = p;
+    } else if (!g_scratch_addr[dev]) {
+      return fail(LGV_ERR_STATE,
+                  "lgv_measure_aos_noalloc: first call on this device made during stream capture; call it once "
+                  "before capturing");
     }
     scratch = g_scratch_addr[dev];
   }
   const size_t table = 25ull * N * N;
-  cudaStream_t st = (cudaStream_t)stream;
   if (lgv::launch_measure_sums_aos(dev_aos, N, scratch, scratch + table, st) != cudaSuccess ||
       lgv::launch_measure_finish(scratch, scratch + table, N, dev_out, st) != cudaSuccess)
     return fail(LGV_ERR_CUDA, "lgv_measure_aos_noalloc: kernel launch failed");

@@ -49,13 +49,16 @@ def unpack(buf, N):
     return out
 
 
-def test_measure_noalloc_matches_measure_on_two_calls(lgv):
+@pytest.mark.parametrize("N", [32, 128])
+def test_measure_noalloc_matches_measure_on_two_calls(lgv, N):
+    """N = 32, and N = LGV_NOALLOC_MAX_N = 128, where the two partial-sum
+    tables fill the static array to its last element."""
     import torch
 
     from langevina_b200 import _lib as L
 
     lib = L.load()
-    N = 32
+    assert N <= L.NOALLOC_MAX_N
     torch.cuda.set_device(0)
     out = torch.empty(int(lib.lgv_measure_size(N)), dtype=torch.float64, device="cuda")
     for call, seed in enumerate((401, 402)):
