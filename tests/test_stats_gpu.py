@@ -129,9 +129,15 @@ def test_heat_bath_equilibrium_is_dt_independent_and_near_hcrit1(lgv):
     """Metropolis with a symmetric proposal of width sqrt(2 dt Gamma) samples
     exp(-S) whatever dt is: two 64-replica ensembles at dt = 0.05 and 0.2
     must agree.  Their pooled <phi_0>, <phi^2> are then set against the
-    hcrit1 golden (columns 1-2 and 13-14)."""
+    equilibrium of the reference's own EulerLangevinHB at the same point
+    (tests/golden/hcrit1_refbuild.json: seven runs of the reference build,
+    tests/golden/make_hcrit_refbuild.py) within 4 sigma, and against the
+    hcrit1 file golden (columns 1-2 and 13-14) within 5 sigma -- the file sits
+    4.0 and 3.3 sigma above the reference's own heat bath too."""
     with open(os.path.join(GOLD, "hcrit1.json")) as f:
         gold = json.load(f)
+    with open(os.path.join(GOLD, "hcrit1_refbuild.json")) as f:
+        ref = json.load(f)
     a = ensemble_hb_equilibrium(lgv, 64, 7000, 0.05)
     b = ensemble_hb_equilibrium(lgv, 64, 9000, 0.2)
     golden = {"phi0": (gold["phi0_mean"], gold["phi0_err"]), "phi2": (0.99771450882, 4.8322472767e-05)}
@@ -144,8 +150,12 @@ def test_heat_bath_equilibrium_is_dt_independent_and_near_hcrit1(lgv):
         e = 1 / math.sqrt(w.sum())
         g, ge = golden[k]
         pull = (m - g) / math.hypot(e, ge)
+        rm, re = ref[k]["mean"], ref[k]["err"]
+        rpull = (m - rm) / math.hypot(e, re)
         print(f"{k}: dt 0.05 {ma:.6f}+-{ea:.6f}, dt 0.2 {mb:.6f}+-{eb:.6f}, pooled {m:.6f}+-{e:.6f}, "
-              f"golden {g:.6f}+-{ge:.6f}, pull {pull:+.2f}")
+              f"reference build {rm:.6f}+-{re:.6f} (pull {rpull:+.2f}), file golden {g:.6f}+-{ge:.6f} "
+              f"(pull {pull:+.2f})")
+        assert abs(rpull) < 4
         assert abs(pull) < 5
 
 
