@@ -1241,7 +1241,7 @@ __device__ __forceinline__ void em_pair(const Fields &in, const Fields &out, con
 // flat over the V/2 pairs.  AVG: also the volume averages of the new phi into
 // avg_out[0..3] (grid_sum4).
 template <bool INJECTED, bool AVG>
-__global__ void __launch_bounds__(kThreads) em_kernel(Fields in, Fields out, Geo g, EmArgs a, double *partial,
+__global__ void __launch_bounds__(kThreads, 4) em_kernel(Fields in, Fields out, Geo g, EmArgs a, double *partial,
                                                       unsigned *done, double *avg_out) {
   const long long idx = (long long)blockIdx.x * kThreads + threadIdx.x;
   double acc[4] = {0, 0, 0, 0};
