@@ -323,6 +323,54 @@ int lgv_ensemble_synchronize(lgv_ensemble *e);
 #define LGV_NOALLOC_MAX_N 128
 int lgv_measure_aos_noalloc(const double *dev_aos, int N, double *dev_out, void *stream);
 
+/* ---- Lattices split into z-slabs over ranks (no single
+ * counterpart: it replaces the z-decomposition of DMDACreate3d,
+ * ModelA.h:315-318, with its ghost exchanges DMGlobalToLocal before every
+ * pass, Stepper.cxx:81-82, 312-315, 477-480).
+ *
+ * lgv_slab_create makes a handle for global planes k0 .. k0+nz-1 of the N^3
+ * lattice of `params` (k0 and nz even, nz >= 2), held with two ghost planes on
+ * each side: its buffers are N x N x (nz + 4) sites, local plane 0 being global
+ * plane k0 - 2 (mod N).  lgv_step then advances the slab exactly as a whole
+ * lattice would advance those planes -- the same counter streams, indexed by
+ * the global site -- provided that before every sub-pass that reads across
+ * planes (each ideal step, each phi parity pass, each z-face of the charge
+ * heat bath, each Euler-Maruyama step) the ghost planes hold the neighbours'
+ * current values.  lgv_step calls the halo function set by lgv_slab_set_halo
+ * at those points, from the calling thread, with the component groups to
+ * refresh (LGV_HALO_PHI, LGV_HALO_CHARGES or both); it returns 0 on success.
+ * The function packs this slab's two lowest and two highest planes
+ * (lgv_slab_pack, side 0 / 1), sends them to the rank below / above (global
+ * planes wrap), and unpacks what it receives from the rank below into side 0
+ * and from the rank above into side 1 (lgv_slab_unpack).  Pack and unpack are
+ * asynchronous on the handle's stream; the halo function synchronises it
+ * before handing buffers to another stream or process.  A buffer holds
+ * lgv_slab_halo_doubles(h, comps) doubles.
+ *
+ * lgv_set_state / lgv_get_state (and the _device forms) move the whole
+ * buffer, ghosts included: N x N x (nz + 4) x 10 doubles, u[k][j][i][L] with k
+ * the local plane.  Counter noise only; initialisation, injected noise,
+ * per-site flags, accept statistics, energies and the differentiable runs are
+ * refused (LGV_ERR_UNSUPPORTED).
+ *
+ * Measurement: lgv_slab_measure_partials writes this slab's rows of
+ * T[25][N][N] (T[o][k][i] = sum_j obs, rows k0 .. k0+nz-1; other rows are not
+ * touched) and U[25][N][N] (U[o][j][i] = sum over this slab's planes of obs),
+ * device memory, asynchronous.  Summing every rank's T (zero elsewhere) and U
+ * and calling lgv_measure_from_partials gives lgv_measure_device's output for
+ * the whole lattice. */
+#define LGV_HALO_PHI 1
+#define LGV_HALO_CHARGES 2
+#define LGV_HALO_ALL 3
+typedef int (*lgv_halo_fn)(void *ctx, lgv_handle *h, int comps);
+int lgv_slab_create(const lgv_params *params, int k0, int nz, lgv_handle **out);
+int lgv_slab_set_halo(lgv_handle *h, lgv_halo_fn fn, void *ctx);
+size_t lgv_slab_halo_doubles(lgv_handle *h, int comps);
+int lgv_slab_pack(lgv_handle *h, int side, int comps, double *dev_buf);
+int lgv_slab_unpack(lgv_handle *h, int side, int comps, const double *dev_buf);
+int lgv_slab_measure_partials(lgv_handle *h, double *dev_T, double *dev_U);
+int lgv_measure_from_partials(const double *dev_T, const double *dev_U, int N, double *dev_out, void *stream);
+
 /* Post-processing of measurement histories held in device memory.  Stateless,
  * asynchronous on `stream` (NULL = legacy default stream), no allocation,
  * deterministic (every sum in a fixed order).

@@ -13,6 +13,9 @@ LIB_PATH = os.path.join(HERE, "liblgv.so")
 
 LGV_OK = 0
 LGV_ERR_INVALID, LGV_ERR_CUDA, LGV_ERR_NOMEM, LGV_ERR_TIMEOUT, LGV_ERR_STATE, LGV_ERR_UNSUPPORTED = -1, -2, -3, -4, -5, -6
+HALO_PHI, HALO_CHARGES, HALO_ALL = 1, 2, 3
+# int (*lgv_halo_fn)(void *ctx, lgv_handle *h, int comps)
+HALO_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_int)
 NPHI, NA, NV, NDOF = 4, 3, 3, 10
 NOBS, NOBS_PHASE = 11, 14
 NOALLOC_MAX_N = 128
@@ -105,6 +108,13 @@ SIGNATURES = [
     ("lgv_ensemble_diff_backward", C.c_int, [_H, C.c_void_p, C.c_void_p]),
     ("lgv_ensemble_set_stream", C.c_int, [_H, C.c_void_p]),
     ("lgv_ensemble_synchronize", C.c_int, [_H]),
+    ("lgv_slab_create", C.c_int, [C.POINTER(lgv_params), C.c_int, C.c_int, C.POINTER(_H)]),
+    ("lgv_slab_set_halo", C.c_int, [_H, C.c_void_p, C.c_void_p]),
+    ("lgv_slab_halo_doubles", C.c_size_t, [_H, C.c_int]),
+    ("lgv_slab_pack", C.c_int, [_H, C.c_int, C.c_int, C.c_void_p]),
+    ("lgv_slab_unpack", C.c_int, [_H, C.c_int, C.c_int, C.c_void_p]),
+    ("lgv_slab_measure_partials", C.c_int, [_H, C.c_void_p, C.c_void_p]),
+    ("lgv_measure_from_partials", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     ("lgv_x2k", C.c_int, [C.c_void_p, C.c_int64, C.c_int, C.c_void_p, C.c_void_p]),
     ("lgv_x2k_rotated", C.c_int, [C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
     ("lgv_time_correlator", C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_int, C.c_int,

@@ -106,6 +106,15 @@ struct lgv_handle {
   // lgv_create; the default is lgv::kWaitLimit)
   unsigned long long *waits_dev = nullptr;
   int wait_limit = lgv::kWaitLimit;
+  // Geometry of the buffers: the whole lattice, or for a slab handle
+  // (lgv_slab_create) its planes k0 .. k0+nz-1 with two ghost planes on each
+  // side, filled by the caller's halo exchange before every sub-pass that
+  // reads across planes.
+  lgv::Geo geo{};
+  bool slab = false;
+  int k0 = 0, nz = 0;
+  lgv_halo_fn halo_fn = nullptr;
+  void *halo_ctx = nullptr;
   // charge heat bath as three two-face launches (one per direction) instead
   // of six single-face launches (LGV_CHARGE_FUSED=1 at lgv_create)
   bool charge_per_face = true;
@@ -170,6 +179,20 @@ int check_waits(lgv_handle *h) {
                 "is not valid",
                 n, m);
   return LGV_OK;
+}
+
+// Slab handles: ask the caller's exchange to fill the ghost planes of the
+// current buffer for the component groups `comps` (LGV_HALO_*).
+int halo(lgv_handle *h, int comps) {
+  if (!h->slab) return LGV_OK;
+  if (!h->halo_fn) return fail(LGV_ERR_STATE, "slab handle has no halo exchange (lgv_slab_set_halo)");
+  const int r = h->halo_fn(h->halo_ctx, h, comps);
+  if (r != 0) return fail(LGV_ERR_STATE, "halo exchange failed (%d)", r);
+  return LGV_OK;
+}
+
+int no_slab(lgv_handle *h, const char *what) {
+  return h->slab ? fail(LGV_ERR_UNSUPPORTED, "%s: not available on a slab handle", what) : LGV_OK;
 }
 
 int ensure_scratch(lgv_handle *h, size_t n) {
@@ -259,9 +282,10 @@ int sub_ideal(lgv_handle *h, double dt) {  // IdealPV2::step (Stepper.cxx:23-66)
   a.H = h->p.H;
   a.waits = h->waits_dev;
   a.wait_limit = h->wait_limit;
+  LGV_TRY(halo(h, LGV_HALO_ALL));
   {
     KTimer tm(h, LGV_KCLASS_IDEAL);
-    LGV_CK(lgv::launch_ideal(h->cur, h->alt, h->N, a, h->stream));
+    LGV_CK(lgv::launch_ideal(h->cur, h->alt, h->geo, a, h->stream));
   }
   std::swap(h->cur, h->alt);
   if (h->mon_on) {
@@ -303,8 +327,10 @@ int sub_hb(lgv_handle *h, double dt, double mass) {  // EulerLangevinHB::step (S
     for (int l = 0; l < 4; ++l) std::swap(h->cur.c[l], h->alt.c[l]);
   } else {
     for (int parity = 0; parity < 2; ++parity) {
+      LGV_TRY(halo(h, LGV_HALO_PHI));
       KTimer tm(h, LGV_KCLASS_PHI_HB);
-      LGV_CK(lgv::launch_hb_pass(h->cur, h->N, parity, a, h->stream));
+      if (h->slab) LGV_CK(lgv::launch_hb_pass(h->cur, h->geo, parity, a, h->stream));
+      else LGV_CK(lgv::launch_hb_pass(h->cur, h->N, parity, a, h->stream));
     }
   }
   if (h->noise_mode == LGV_NOISE_INJECTED) h->have_hb = false;
@@ -371,8 +397,9 @@ int sub_charge(lgv_handle *h, double dt) {  // ModelGChargeHB::step (Stepper.cxx
     for (int p = 0; p < 6; ++p) {
       a.pass = p;
       if (h->noise_mode != LGV_NOISE_INJECTED) a.sk = lgv::sub_key(h->key, h->ctr + 1 + p);
+      if (xyz[p / 2] == 2) LGV_TRY(halo(h, LGV_HALO_CHARGES));  // links across planes
       KTimer tm(h, LGV_KCLASS_CHARGE);
-      LGV_CK(lgv::launch_charge_pass(h->cur, h->N, xyz[p / 2], eo[p % 2], a, h->stream));
+      LGV_CK(lgv::launch_charge_pass(h->cur, h->geo, xyz[p / 2], eo[p % 2], a, h->stream));
     }
   } else {
     // both faces of a direction per launch (same streams and order as per face)
@@ -414,9 +441,10 @@ int sub_em(lgv_handle *h, double dt, double mass) {
   } else {
     a.sk = lgv::sub_key(h->key, h->ctr);
   }
+  LGV_TRY(halo(h, LGV_HALO_PHI));
   {
     KTimer tm(h, LGV_KCLASS_EM);
-    LGV_CK(lgv::launch_em(h->cur, h->alt, h->N, a, h->stream));
+    LGV_CK(lgv::launch_em(h->cur, h->alt, h->geo, a, h->stream));
   }
   for (int l = 0; l < 4; ++l) std::swap(h->cur.c[l], h->alt.c[l]);
   if (h->noise_mode == LGV_NOISE_INJECTED) h->have_em = false;
@@ -480,19 +508,22 @@ const char *lgv_status_string(int s) {
 
 const char *lgv_last_error(void) { return g_last_error.c_str(); }
 
-int lgv_create(const lgv_params *params, lgv_handle **out) {
-  if (!out) return fail(LGV_ERR_INVALID, "out is NULL");
-  *out = nullptr;
-  LGV_TRY(check_params(params));
+namespace {
+// Shared by lgv_create and lgv_slab_create: buffers for geometry g.
+int create_handle(const lgv_params *params, const lgv::Geo &g, bool slab, int k0, int nz, lgv_handle **out) {
   int dev = 0;
   LGV_CK(cudaGetDevice(&dev));
   lgv_handle *h = new lgv_handle();
   h->p = *params;
   h->N = params->N;
-  h->V = (size_t)h->N * h->N * h->N;
+  h->geo = g;
+  h->V = (size_t)(2 * g.V2);
+  h->slab = slab;
+  h->k0 = k0;
+  h->nz = nz;
   h->device = dev;
   h->key = lgv::make_key(params->seed);
-  {
+  if (!slab) {
     const char *f = std::getenv("LGV_HB_FUSED");
     h->hb_fused = f && f[0] == '1';
     // one face per launch (the faster path on B200); LGV_CHARGE_FUSED=1 selects
@@ -511,6 +542,8 @@ int lgv_create(const lgv_params *params, lgv_handle **out) {
       h->hb_fuse = fuse;
     }
     if (h->hb_fused) h->hb_ordered = false;
+  }
+  {
     const char *wl = std::getenv("LGV_WAIT_LIMIT");
     if (wl && wl[0]) h->wait_limit = std::max(0, std::atoi(wl));
   }
@@ -549,6 +582,88 @@ int lgv_create(const lgv_params *params, lgv_handle **out) {
     return rc;
   }
   *out = h;
+  return LGV_OK;
+}
+}  // namespace
+
+int lgv_create(const lgv_params *params, lgv_handle **out) {
+  if (!out) return fail(LGV_ERR_INVALID, "out is NULL");
+  *out = nullptr;
+  LGV_TRY(check_params(params));
+  return create_handle(params, lgv::make_geo(params->N), false, 0, 0, out);
+}
+
+int lgv_slab_create(const lgv_params *params, int k0, int nz, lgv_handle **out) {
+  if (!out) return fail(LGV_ERR_INVALID, "out is NULL");
+  *out = nullptr;
+  LGV_TRY(check_params(params));
+  const int N = params->N;
+  if (nz < 2 || (nz & 1) || k0 < 0 || (k0 & 1) || k0 + nz > N)
+    return fail(LGV_ERR_INVALID, "slab planes [%d, %d): need k0 even, nz even >= 2, k0 + nz <= N = %d", k0, k0 + nz, N);
+  return create_handle(params, lgv::make_slab_geo(N, nz + 4, k0 - 2), true, k0, nz, out);
+}
+
+int lgv_slab_set_halo(lgv_handle *h, lgv_halo_fn fn, void *ctx) {
+  if (!h) return fail(LGV_ERR_INVALID, "handle is NULL");
+  if (!h->slab) return fail(LGV_ERR_INVALID, "not a slab handle");
+  h->halo_fn = fn;
+  h->halo_ctx = ctx;
+  return LGV_OK;
+}
+
+size_t lgv_slab_halo_doubles(lgv_handle *h, int comps) {
+  if (!h || !h->slab) return 0;
+  const int nc = ((comps & LGV_HALO_PHI) ? 4 : 0) + ((comps & LGV_HALO_CHARGES) ? 6 : 0);
+  return (size_t)nc * 2 * 2 * h->N * (h->N / 2);
+}
+
+namespace {
+// The two planes of side `side` (0 below, 1 above) of the current buffer:
+// interior planes to send (ghost = false) or ghost planes to fill (true), as
+// per (component, parity half) runs of 2 N^2/2 contiguous doubles.
+int slab_copy(lgv_handle *h, int side, int comps, double *buf, bool unpack) {
+  if (!h || !buf) return fail(LGV_ERR_INVALID, "NULL argument");
+  if (!h->slab) return fail(LGV_ERR_INVALID, "not a slab handle");
+  if ((side != 0 && side != 1) || comps < 1 || comps > LGV_HALO_ALL) return fail(LGV_ERR_INVALID, "side/comps");
+  DeviceGuard g(h->device);
+  const size_t run = (size_t)2 * h->N * (h->N / 2);  // two planes of one parity half
+  int plane;
+  if (unpack) plane = side == 0 ? 0 : h->nz + 2;
+  else plane = side == 0 ? 2 : h->nz;
+  const size_t off = (size_t)plane * h->N * (h->N / 2);
+  size_t q = 0;
+  for (int c = 0; c < 10; ++c) {
+    if (!((c < 4 && (comps & LGV_HALO_PHI)) || (c >= 4 && (comps & LGV_HALO_CHARGES)))) continue;
+    for (int par = 0; par < 2; ++par) {
+      double *field = h->cur.c[c] + (size_t)par * h->geo.V2 + off;
+      if (unpack)
+        LGV_CK(cudaMemcpyAsync(field, buf + q, run * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+      else
+        LGV_CK(cudaMemcpyAsync(buf + q, field, run * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+      q += run;
+    }
+  }
+  return LGV_OK;
+}
+}  // namespace
+
+int lgv_slab_pack(lgv_handle *h, int side, int comps, double *dev_buf) { return slab_copy(h, side, comps, dev_buf, false); }
+int lgv_slab_unpack(lgv_handle *h, int side, int comps, const double *dev_buf) {
+  return slab_copy(h, side, comps, const_cast<double *>(dev_buf), true);
+}
+
+int lgv_slab_measure_partials(lgv_handle *h, double *dev_T, double *dev_U) {
+  if (!h || !dev_T || !dev_U) return fail(LGV_ERR_INVALID, "NULL argument");
+  if (!h->slab) return fail(LGV_ERR_INVALID, "not a slab handle");
+  DeviceGuard g(h->device);
+  LGV_CK(lgv::launch_measure_partials(h->cur, h->geo, 2, h->nz, h->k0, dev_T, dev_U, h->stream));
+  return LGV_OK;
+}
+
+int lgv_measure_from_partials(const double *dev_T, const double *dev_U, int N, double *dev_out, void *stream) {
+  if (!dev_T || !dev_U || !dev_out) return fail(LGV_ERR_INVALID, "NULL argument");
+  if (N < 4 || (N & 1)) return fail(LGV_ERR_INVALID, "N must be even and >= 4");
+  LGV_CK(lgv::launch_measure_finish(dev_T, dev_U, N, dev_out, (cudaStream_t)stream));
   return LGV_OK;
 }
 
@@ -591,7 +706,7 @@ int lgv_set_state(lgv_handle *h, const double *host_aos) {
   DeviceGuard g(h->device);
   LGV_TRY(ensure(&h->staging, 10 * h->V));
   LGV_CK(cudaMemcpyAsync(h->staging, host_aos, 10 * h->V * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-  LGV_CK(lgv::launch_aos_to_rb(h->staging, h->cur, h->N, h->stream));
+  LGV_CK(lgv::launch_aos_to_rb(h->staging, h->cur, h->geo, h->stream));
   LGV_CK(cudaStreamSynchronize(h->stream));
   return LGV_OK;
 }
@@ -600,7 +715,7 @@ int lgv_get_state(lgv_handle *h, double *host_aos) {
   if (!h || !host_aos) return fail(LGV_ERR_INVALID, "NULL argument");
   DeviceGuard g(h->device);
   LGV_TRY(ensure(&h->staging, 10 * h->V));
-  LGV_CK(lgv::launch_rb_to_aos(h->cur, h->staging, h->N, h->stream));
+  LGV_CK(lgv::launch_rb_to_aos(h->cur, h->staging, h->geo, h->stream));
   LGV_CK(cudaMemcpyAsync(host_aos, h->staging, 10 * h->V * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   LGV_CK(cudaStreamSynchronize(h->stream));
   return check_waits(h);
@@ -609,19 +724,20 @@ int lgv_get_state(lgv_handle *h, double *host_aos) {
 int lgv_set_state_device(lgv_handle *h, const double *dev_aos) {
   if (!h || !dev_aos) return fail(LGV_ERR_INVALID, "NULL argument");
   DeviceGuard g(h->device);
-  LGV_CK(lgv::launch_aos_to_rb(dev_aos, h->cur, h->N, h->stream));
+  LGV_CK(lgv::launch_aos_to_rb(dev_aos, h->cur, h->geo, h->stream));
   return LGV_OK;
 }
 
 int lgv_get_state_device(lgv_handle *h, double *dev_aos) {
   if (!h || !dev_aos) return fail(LGV_ERR_INVALID, "NULL argument");
   DeviceGuard g(h->device);
-  LGV_CK(lgv::launch_rb_to_aos(h->cur, dev_aos, h->N, h->stream));
+  LGV_CK(lgv::launch_rb_to_aos(h->cur, dev_aos, h->geo, h->stream));
   return LGV_OK;
 }
 
 int lgv_initialize(lgv_handle *h, int kind, double scale) {
   if (!h) return fail(LGV_ERR_INVALID, "handle is NULL");
+  LGV_TRY(no_slab(h, "lgv_initialize"));
   DeviceGuard g(h->device);
   switch (kind) {
     case LGV_INIT_ZERO:
@@ -646,6 +762,7 @@ int lgv_initialize(lgv_handle *h, int kind, double scale) {
 int lgv_set_noise_mode(lgv_handle *h, int mode) {
   if (!h) return fail(LGV_ERR_INVALID, "handle is NULL");
   if (mode != LGV_NOISE_COUNTER && mode != LGV_NOISE_INJECTED) return fail(LGV_ERR_INVALID, "noise mode %d", mode);
+  if (mode == LGV_NOISE_INJECTED) LGV_TRY(no_slab(h, "injected noise"));
   h->noise_mode = mode;
   return LGV_OK;
 }
@@ -714,6 +831,7 @@ size_t lgv_measure_size(int N) { return lgv::measure_size(N); }
 
 int lgv_measure_device(lgv_handle *h, double *dev_out) {
   if (!h || !dev_out) return fail(LGV_ERR_INVALID, "NULL argument");
+  LGV_TRY(no_slab(h, "lgv_measure_device (use lgv_slab_measure_partials)"));
   DeviceGuard g(h->device);
   LGV_TRY(ensure_scratch(h, lgv::measure_scratch_doubles(h->N)));
   KTimer tm(h, LGV_KCLASS_MEASURE);
@@ -747,12 +865,14 @@ int lgv_measure(lgv_handle *h, lgv_measurement *out) {
 
 int lgv_energy(lgv_handle *h, double *energy) {
   if (!h || !energy) return fail(LGV_ERR_INVALID, "NULL argument");
+  LGV_TRY(no_slab(h, "lgv_energy"));
   DeviceGuard g(h->device);
   return energy_now(h, energy);
 }
 
 int lgv_enable_monitors(lgv_handle *h, int enable) {
   if (!h) return fail(LGV_ERR_INVALID, "handle is NULL");
+  if (enable) LGV_TRY(no_slab(h, "accept statistics"));
   DeviceGuard g(h->device);
   h->mon_on = enable != 0;
   h->mon_ideal = lgv_monitor{};
@@ -908,6 +1028,7 @@ bool has_em(int ev) { return ev == LGV_MODELA_EM || ev == LGV_IDEAL_EM; }
 int lgv_diff_forward(lgv_handle *h, int evolver, double dt, double t, int nsteps, int avg_begin, int ckpt_every,
                      double *obs) {
   if (!h || !obs) return fail(LGV_ERR_INVALID, "NULL argument");
+  LGV_TRY(no_slab(h, "lgv_diff_forward"));
   if (!has_ideal(evolver) && !has_em(evolver))
     return fail(LGV_ERR_INVALID, "lgv_diff_forward: evolver %d has no adjoint (LGV_MODELA_EM, LGV_IDEAL_PV2, LGV_IDEAL_EM)",
                 evolver);
@@ -1089,6 +1210,7 @@ int lgv_diff_backward(lgv_handle *h, const double *w, double *grad) {
 
 int lgv_debug_flags(lgv_handle *h, int enable) {
   if (!h) return fail(LGV_ERR_INVALID, "handle is NULL");
+  if (enable) LGV_TRY(no_slab(h, "per-site flags"));
   DeviceGuard g(h->device);
   if (enable) {
     if (!h->flags_dev) {

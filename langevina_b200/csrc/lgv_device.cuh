@@ -20,10 +20,17 @@ struct Fields {
 };
 
 // Geometry helpers -----------------------------------------------------------
+// A buffer holds Nz planes of N x N sites.  For a whole lattice Nz = N; a
+// z-slab of a lattice split over ranks holds its own planes plus ghost planes,
+// local plane 0 being global plane kg (even, so the checkerboard parity of a
+// local site is that of its global site) of the Ng-plane lattice.
 struct Geo {
-  int N;      // lattice extent
-  int H;      // N / 2
-  long long V2;  // V / 2
+  int N;         // lattice extent in x and y
+  int H;         // N / 2
+  long long V2;  // sites of one parity in the buffer: N * N * Nz / 2
+  int Nz;        // planes in the buffer
+  int kg;        // global plane of local plane 0 (0 for a whole lattice)
+  int Ng;        // planes of the whole lattice (N)
 };
 
 __host__ __device__ __forceinline__ Geo make_geo(int N) {
@@ -31,8 +38,29 @@ __host__ __device__ __forceinline__ Geo make_geo(int N) {
   g.N = N;
   g.H = N >> 1;
   g.V2 = (long long)N * N * (N >> 1);
+  g.Nz = N;
+  g.kg = 0;
+  g.Ng = N;
   return g;
 }
+
+__host__ __device__ __forceinline__ Geo make_slab_geo(int N, int Nz, int kg) {
+  Geo g = make_geo(N);
+  g.V2 = (long long)N * N * Nz / 2;
+  g.Nz = Nz;
+  g.kg = kg;
+  return g;
+}
+
+// Natural index of the global site of local site (i, j, k): the noise streams,
+// injected arrays and per-site flags are indexed by it.
+__host__ __device__ __forceinline__ long long nat_index(const Geo &g, int i, int j, int k) {
+  int kk = k + g.kg;
+  if (kk < 0) kk += g.Ng;
+  else if (kk >= g.Ng) kk -= g.Ng;
+  return ((long long)kk * g.N + j) * g.N + i;
+}
+__host__ __device__ __forceinline__ long long global_sites(const Geo &g) { return (long long)g.N * g.N * g.Ng; }
 
 // red-black offset of natural site (i, j, k) inside a component plane
 __host__ __device__ __forceinline__ long long rb_off(const Geo &g, int i, int j, int k) {

@@ -20,6 +20,7 @@
 
 #include <map>
 #include <mutex>
+#include <tuple>
 #include <utility>
 
 #include "lgv_internal.h"
@@ -115,7 +116,7 @@ __device__ __forceinline__ void ideal_tma_cta(const CUtensorMap *maps, const Fie
   const int lx = 2 * t + hw;  // each half warp owns one x-parity of the row
   const int x0 = bx * TX, y0 = by * TY;
   const int z0 = bz * zchunk;
-  const int z1 = min(z0 + zchunk, N);
+  const int z1 = min(z0 + zchunk, g.Nz);
   const int nit = (z1 - z0) + 2;
   const int xi = x0 + lx, yj = y0 + ty;
   const unsigned bar0 = smem_addr(&mbar[0]);  // stage s uses bar0 + 8 s
@@ -143,7 +144,7 @@ __device__ __forceinline__ void ideal_tma_cta(const CUtensorMap *maps, const Fie
   // z-1 neighbour and needs no ring) goes to stage q % NS; one cp.async group
   // per plane, possibly empty, so waiting for all groups covers plane q.
   auto issue = [&](int q) {
-    const int pl = wrapn(z0 - 1 + q, N), sn = q % NS;
+    const int pl = wrapn(z0 - 1 + q, g.Nz), sn = q % NS;
     if (tid == 0) issue_plane(maps, core + sn * 10 * CORE, bar0 + 8 * sn, x0 / 2, y0, pl);
     if (ring && q >= 1) {
       const long long oh = rb_off(g, hxg, hyg, pl);
@@ -159,7 +160,7 @@ __device__ __forceinline__ void ideal_tma_cta(const CUtensorMap *maps, const Fie
   double pm[4], pc[4], pn[4], qc[6], qn[6];
   unsigned wbar = bar0, wpar = 0;  // the barrier phase waited on last
   for (int it = 0; it < nit; ++it) {
-    const int p = wrapn(z0 - 1 + it, N);
+    const int p = wrapn(z0 - 1 + it, g.Nz);
     const int st = it % NS;
     wbar = bar0 + 8 * st;
     wpar = (unsigned)((it / NS) & 1);
@@ -202,7 +203,7 @@ __device__ __forceinline__ void ideal_tma_cta(const CUtensorMap *maps, const Fie
       // phi' of plane p-1, written last iteration; the barrier at the top of
       // this iteration also ends last iteration's reads of the buffer written now
       const double *pp = phs + ((it + 1) & 1) * 4 * PH;
-      const int kk = wrapn(p - 1, N);
+      const int kk = wrapn(p - 1, g.Nz);
       const int nh = ((hw + y0 + ty + kk) & 1) ^ 1;  // the neighbours' half
       const int rx = (nh * PR + ty + 1) * PM;
       const int oxp = rx + t + 1 + hw, oxm = rx + t + hw;
@@ -303,11 +304,11 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   return fn;
 }
 
-bool plane_map(const double *plane, int N, CUtensorMap *out) {
+bool plane_map(const double *plane, int N, int Nz, CUtensorMap *out) {
   static std::mutex mu;
-  static std::map<std::pair<const double *, int>, CUtensorMap> cache;
+  static std::map<std::tuple<const double *, int, int>, CUtensorMap> cache;
   std::lock_guard<std::mutex> lk(mu);
-  auto it = cache.find({plane, N});
+  auto it = cache.find({plane, N, Nz});
   if (it != cache.end()) {
     *out = it->second;
     return true;
@@ -315,8 +316,8 @@ bool plane_map(const double *plane, int N, CUtensorMap *out) {
   auto fn = encode_fn();
   if (!fn) return false;
   const cuuint64_t H = (cuuint64_t)(N / 2);
-  const cuuint64_t dims[4] = {H, (cuuint64_t)N, (cuuint64_t)N, 2};
-  const cuuint64_t strides[3] = {H * 8, (cuuint64_t)N * H * 8, (cuuint64_t)N * N * H * 8};
+  const cuuint64_t dims[4] = {H, (cuuint64_t)N, (cuuint64_t)Nz, 2};
+  const cuuint64_t strides[3] = {H * 8, (cuuint64_t)N * H * 8, (cuuint64_t)N * Nz * H * 8};
   const cuuint32_t box[4] = {HM, TY, 1, 2};
   const cuuint32_t estr[4] = {1, 1, 1, 1};
   CUtensorMap m;
@@ -325,7 +326,7 @@ bool plane_map(const double *plane, int N, CUtensorMap *out) {
          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
     return false;
   if (cache.size() > 4096) cache.clear();
-  cache.emplace(std::make_pair(plane, N), m);
+  cache.emplace(std::make_tuple(plane, N, Nz), m);
   *out = m;
   return true;
 }
@@ -336,17 +337,17 @@ bool ideal_tma_supported(int N) {
   return N >= 32 && N % 32 == 0 && encode_fn() != nullptr;
 }
 
-cudaError_t launch_ideal_tma(Fields in, Fields out, int N, int zchunk, const IdealArgs &a, cudaStream_t st) {
+cudaError_t launch_ideal_tma(Fields in, Fields out, const Geo &g, int zchunk, const IdealArgs &a, cudaStream_t st) {
+  const int N = g.N;
   if (!ideal_tma_supported(N)) return cudaErrorInvalidValue;
   for (int c = 0; c < 10; ++c)
     if (((uintptr_t)in.c[c] & 15) != 0) return cudaErrorMisalignedAddress;
   TmaMaps maps;
   for (int c = 0; c < 10; ++c)
-    if (!plane_map(in.c[c], N, &maps.m[c])) return cudaErrorInvalidValue;
+    if (!plane_map(in.c[c], N, g.Nz, &maps.m[c])) return cudaErrorInvalidValue;
   cudaError_t e = cudaFuncSetAttribute(ideal_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
   if (e != cudaSuccess) return e;
-  const Geo g = make_geo(N);
-  dim3 grid(N / TX, N / TY, (unsigned)((N + zchunk - 1) / zchunk));
+  dim3 grid(N / TX, N / TY, (unsigned)((g.Nz + zchunk - 1) / zchunk));
   ideal_tma_kernel<<<grid, NT, kSmemBytes, st>>>(maps, in, out, g, zchunk, a);
   return cudaGetLastError();
 }
@@ -355,7 +356,7 @@ int batch_tma_blocks(int N, int zchunk) { return (N / TX) * (N / TY) * ((N + zch
 
 bool tma_plane_map(const double *plane, int N, void *out128) {
   if (((uintptr_t)plane & 15) != 0) return false;
-  return plane_map(plane, N, reinterpret_cast<CUtensorMap *>(out128));
+  return plane_map(plane, N, N, reinterpret_cast<CUtensorMap *>(out128));
 }
 
 cudaError_t launch_batch_ideal_tma(const RepDesc *d, const void *gmaps, const int *rep, const int *first, int nblocks,

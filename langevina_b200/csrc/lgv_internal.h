@@ -191,11 +191,15 @@ cudaError_t launch_fill_phi(Fields f, int N, const double v[4], cudaStream_t st)
 // Launchers (lgv_kernels.cu).  All asynchronous on `st`; return cudaError_t.
 cudaError_t launch_aos_to_rb(const double *aos, Fields f, int N, cudaStream_t st);
 cudaError_t launch_rb_to_aos(Fields f, double *aos, int N, cudaStream_t st);
+// The same for a buffer of any geometry (a z-slab with ghost planes).
+cudaError_t launch_aos_to_rb(const double *aos, Fields f, const Geo &g, cudaStream_t st);
+cudaError_t launch_rb_to_aos(Fields f, double *aos, const Geo &g, cudaStream_t st);
 cudaError_t launch_init_phi(Fields f, int N, uint64_t sk, double scale, cudaStream_t st);
 cudaError_t launch_init_charges(Fields f, int N, uint64_t sk, double sqrtchi, double *scratch,
                                 cudaStream_t st);
 // one phi heat-bath parity pass, in place
 cudaError_t launch_hb_pass(Fields f, int N, int parity, const HbArgs &a, cudaStream_t st);
+cudaError_t launch_hb_pass(Fields f, const Geo &g, int parity, const HbArgs &a, cudaStream_t st);
 // Ordered phi sweeps (hb_ordered_kernel): one persistent launch runs 1 ..
 // kHbMaxSweeps whole sweeps in place, z-slab by z-slab.  A plan holds the
 // chunk schedule for each sweep count and the launch's counters; it is built
@@ -221,6 +225,7 @@ cudaError_t hb_plan_timeouts(const HbPlan &plan, cudaStream_t st, unsigned long 
 // one full phi heat-bath sweep (both parities, z-marching): reads phi of `in`, writes phi of `out`
 cudaError_t launch_hb_sweep(Fields in, Fields out, int N, const HbArgs &a, cudaStream_t st);
 cudaError_t launch_charge_pass(Fields f, int N, int dir, int eoA, const ChargeArgs &a, cudaStream_t st);
+cudaError_t launch_charge_pass(Fields f, const Geo &g, int dir, int eoA, const ChargeArgs &a, cudaStream_t st);
 // Both faces of direction dir.  x runs in place on `in`; y and z read `in`
 // and write the charges of `out` (*swapped = true: the caller swaps the
 // charge planes).
@@ -230,9 +235,11 @@ cudaError_t launch_charge_dir(Fields in, Fields out, int N, int dir, const Charg
                               bool *swapped);
 cudaError_t launch_em(Fields in, Fields out, int N, const EmArgs &a, cudaStream_t st);
 cudaError_t launch_ideal(Fields in, Fields out, int N, const IdealArgs &a, cudaStream_t st);
+cudaError_t launch_em(Fields in, Fields out, const Geo &g, const EmArgs &a, cudaStream_t st);
+cudaError_t launch_ideal(Fields in, Fields out, const Geo &g, const IdealArgs &a, cudaStream_t st);
 // TMA-staged ideal step (lgv_ideal_tma.cu): N divisible by 32
 bool ideal_tma_supported(int N);
-cudaError_t launch_ideal_tma(Fields in, Fields out, int N, int zchunk, const IdealArgs &a, cudaStream_t st);
+cudaError_t launch_ideal_tma(Fields in, Fields out, const Geo &g, int zchunk, const IdealArgs &a, cudaStream_t st);
 // Ensembles: the TMA ideal step for replicas with N divisible by 32.
 // tma_plane_map encodes the 128-byte tensor map of one component plane; gmaps
 // holds, per replica r, buffer phases (pphi, pq) and component c, the map at
@@ -256,5 +263,10 @@ cudaError_t launch_measure(Fields f, int N, double *scratch, double *dev_out, cu
 // OAverage, DFT and vev rotation into dev_out (lgv.h packing).
 cudaError_t launch_measure_sums_aos(const double *aos, int N, double *T, double *U, cudaStream_t st);
 cudaError_t launch_measure_finish(const double *T, const double *U, int N, double *dev_out, cudaStream_t st);
+// A slab's share of those sums: T rows of its planes (local planes klo ..
+// klo+nk-1 = global rows kout .. kout+nk-1 of T[25][Ng][N], other rows left as
+// they are) and U summed over those planes only.
+cudaError_t launch_measure_partials(Fields f, const Geo &g, int klo, int nk, int kout, double *T, double *U,
+                                    cudaStream_t st);
 
 }  // namespace lgv

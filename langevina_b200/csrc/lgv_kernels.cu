@@ -330,8 +330,8 @@ __device__ __forceinline__ void hb_site(const Fields &f, const Geo &g, int parit
   const long long row = ((long long)k * N + j) * H;
   const long long rjp = ((long long)k * N + wrap_inc(j, N)) * H;
   const long long rjm = ((long long)k * N + wrap_dec(j, N)) * H;
-  const long long rkp = ((long long)wrap_inc(k, N) * N + j) * H;
-  const long long rkm = ((long long)wrap_dec(k, N) * N + j) * H;
+  const long long rkp = ((long long)wrap_inc(k, g.Nz) * N + j) * H;
+  const long long rkm = ((long long)wrap_dec(k, g.Nz) * N + j) * H;
   const long long own = (long long)parity * g.V2 + row + m;
   const long long ob = (long long)(parity ^ 1) * g.V2;
   double po[4], heff[4];
@@ -343,9 +343,9 @@ __device__ __forceinline__ void hb_site(const Fields &f, const Geo &g, int parit
               (ld_phi<CG>(P + ob + rkp + m) + ld_phi<CG>(P + ob + rkm + m));
     po[l] = ld_phi<CG>(P + own);
   }
-  const long long nat = ((long long)k * N + j) * N + 2 * m + s;
+  const long long nat = nat_index(g, 2 * m + s, j, k);
   HbDecision d;
-  hb_decide<INJECTED>(po, heff, a, nat, 2 * g.V2, d);
+  hb_decide<INJECTED>(po, heff, a, nat, global_sites(g), d);
   if (d.accept) {
 #pragma unroll
     for (int l = 0; l < 4; ++l) f.c[l][own] = d.pn[l];
@@ -376,7 +376,7 @@ __device__ __forceinline__ bool pass_site(const Geo &g, int &m, int &j, int &k) 
 }
 
 __host__ __forceinline__ dim3 pass_grid(const Geo &g, bool rows) {
-  return rows ? dim3(g.H / 128, g.N, g.N) : dim3((unsigned)(((long long)g.N * g.H + 127) / 128), g.N);
+  return rows ? dim3(g.H / 128, g.N, g.Nz) : dim3((unsigned)(((long long)g.N * g.H + 127) / 128), g.Nz);
 }
 
 template <bool INJECTED, bool MON, bool ROWS>
@@ -787,10 +787,10 @@ __device__ __forceinline__ void charge_link_site(const Fields &f, const Geo &g, 
   } else if (dir == 1) {
     offB = ob + ((long long)k * N + wrap_inc(j, N)) * H + m;
   } else {
-    offB = ob + ((long long)wrap_inc(k, N) * N + j) * H + m;
+    offB = ob + ((long long)wrap_inc(k, g.Nz) * N + j) * H + m;
   }
-  const long long nat = ((long long)k * N + j) * N + i;
-  const long long V = 2 * g.V2;
+  const long long nat = nat_index(g, i, j, k);
+  const long long V = global_sites(g);
   WordStream ws{};
   if (!INJECTED) ws = words_at(a.sk, 6 * (uint64_t)nat);
 #pragma unroll
@@ -1197,8 +1197,8 @@ __device__ __forceinline__ void em_pair(const Fields &in, const Fields &out, con
   const long long row = ((long long)k * N + j) * H;
   const long long rjp = ((long long)k * N + wrap_inc(j, N)) * H;
   const long long rjm = ((long long)k * N + wrap_dec(j, N)) * H;
-  const long long rkp = ((long long)wrap_inc(k, N) * N + j) * H;
-  const long long rkm = ((long long)wrap_dec(k, N) * N + j) * H;
+  const long long rkp = ((long long)wrap_inc(k, g.Nz) * N + j) * H;
+  const long long rkm = ((long long)wrap_dec(k, g.Nz) * N + j) * H;
 #pragma unroll
   for (int parity = 0; parity < 2; ++parity) {
     const int s = (parity + j + k) & 1;
@@ -1208,11 +1208,11 @@ __device__ __forceinline__ void em_pair(const Fields &in, const Fields &out, con
     if (xp == H) xp = 0;
     const long long own = (long long)parity * g.V2 + row + m;
     const long long ob = (long long)(parity ^ 1) * g.V2;
-    const long long nat = ((long long)k * N + j) * N + i;
+    const long long nat = nat_index(g, i, j, k);
     double xi[4];
     if (INJECTED) {
 #pragma unroll
-      for (int l = 0; l < 4; ++l) xi[l] = a.xi[(long long)l * 2 * g.V2 + nat];
+      for (int l = 0; l < 4; ++l) xi[l] = a.xi[(long long)l * global_sites(g) + nat];
     } else {
       Xoro rng = stream_at(a.sk, (uint64_t)nat);
       const uint64_t r1 = rng.next(), r2 = rng.next(), r3 = rng.next(), r4 = rng.next();
@@ -1338,7 +1338,7 @@ __device__ __forceinline__ void ideal_tile(const Fields &in, const Fields &out, 
   const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
   const int x0 = bx * TX, y0 = by * TY;
   const int z0 = bz * zchunk;
-  const int z1 = min(z0 + zchunk, N);
+  const int z1 = min(z0 + zchunk, g.Nz);
   const int nit = (z1 - z0) + 2;
   const bool act = (x0 + tx < N) && (y0 + ty < N);
   const int xi = (x0 + tx) % N, yj = (y0 + ty) % N;
@@ -1368,15 +1368,15 @@ __device__ __forceinline__ void ideal_tile(const Fields &in, const Fields &out, 
     }
   };
 
-  issue(wrapn(z0 - 1, N), 0, false);
+  issue(wrapn(z0 - 1, g.Nz), 0, false);
   cp_async_commit();
 
   double pm[4], pc[4], pn[4], qc[6], qn[6];
   for (int it = 0; it < nit; ++it) {
-    const int p = wrapn(z0 - 1 + it, N);
+    const int p = wrapn(z0 - 1 + it, g.Nz);
     cp_async_wait_all();
     __syncthreads();
-    if (it + 1 < nit) issue(wrapn(p + 1, N), (it + 1) & 1, true);
+    if (it + 1 < nit) issue(wrapn(p + 1, g.Nz), (it + 1) & 1, true);
     cp_async_commit();
 
     const double *rw = raw + (it & 1) * 10 * SP;
@@ -1417,7 +1417,7 @@ __device__ __forceinline__ void ideal_tile(const Fields &in, const Fields &out, 
       // second half rotation on a copy: pc (phi') stays the z-1 neighbour of the next plane
       double pf[4] = {pc[0], pc[1], pc[2], pc[3]};
       rotate_site(pf, qc, a.dto2chi);
-      const long long o = rb_off(g, xi, yj, wrapn(p - 1, N));
+      const long long o = rb_off(g, xi, yj, wrapn(p - 1, g.Nz));
 #pragma unroll
       for (int l = 0; l < 4; ++l) out.c[l][o] = pf[l];
 #pragma unroll
@@ -1540,12 +1540,13 @@ __device__ __forceinline__ void load_site(const Fields &f, const Geo &g, int i, 
   for (int L = 0; L < 10; ++L) s[L] = f.c[L][o];
 }
 
-// T[o][k][i] = sum_j obs(i, j, k)
-__global__ void meas_sum_j_kernel(Fields f, Geo g, double *T) {
+// T[o][kout + k - klo][i] = sum_j obs(i, j, k) for local planes k in [klo, klo + nk);
+// T is [25][Ng][N]
+__global__ void meas_sum_j_kernel(Fields f, Geo g, double *T, int klo, int nk, int kout) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int N = g.N;
-  if (t >= (long long)N * N) return;
-  const int i = (int)(t % N), k = (int)(t / N);
+  if (t >= (long long)N * nk) return;
+  const int i = (int)(t % N), kl = (int)(t / N), k = klo + kl;
   double acc[kNObs];
 #pragma unroll
   for (int o = 0; o < kNObs; ++o) acc[o] = 0;
@@ -1556,13 +1557,13 @@ __global__ void meas_sum_j_kernel(Fields f, Geo g, double *T) {
 #pragma unroll
     for (int o = 0; o < kNObs; ++o) acc[o] += ob[o];
   }
-  const long long NN = (long long)N * N;
+  const long long NT = (long long)g.Ng * N;
 #pragma unroll
-  for (int o = 0; o < kNObs; ++o) T[o * NN + (long long)k * N + i] = acc[o];
+  for (int o = 0; o < kNObs; ++o) T[o * NT + (long long)(kout + kl) * N + i] = acc[o];
 }
 
-// U[o][j][i] = sum_k obs(i, j, k)
-__global__ void meas_sum_k_kernel(Fields f, Geo g, double *U) {
+// U[o][j][i] = sum_k obs(i, j, k) over local planes [klo, klo + nk)
+__global__ void meas_sum_k_kernel(Fields f, Geo g, double *U, int klo, int nk) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int N = g.N;
   if (t >= (long long)N * N) return;
@@ -1570,7 +1571,7 @@ __global__ void meas_sum_k_kernel(Fields f, Geo g, double *U) {
   double acc[kNObs];
 #pragma unroll
   for (int o = 0; o < kNObs; ++o) acc[o] = 0;
-  for (int k = 0; k < N; ++k) {
+  for (int k = klo; k < klo + nk; ++k) {
     double s[10], ob[kNObs];
     load_site(f, g, i, j, k, s);
     site_obs(s, ob);
@@ -2300,16 +2301,20 @@ inline unsigned nblocks(long long n, int bs) { return (unsigned)((n + bs - 1) / 
 
 // ============================================================================
 // Launchers.
-cudaError_t launch_aos_to_rb(const double *aos, Fields f, int N, cudaStream_t st) {
-  const Geo g = make_geo(N);
+cudaError_t launch_aos_to_rb(const double *aos, Fields f, const Geo &g, cudaStream_t st) {
   aos_to_rb_kernel<<<nblocks(2 * g.V2, kThreads), kThreads, 0, st>>>(aos, f, g);
   return cudaGetLastError();
 }
+cudaError_t launch_aos_to_rb(const double *aos, Fields f, int N, cudaStream_t st) {
+  return launch_aos_to_rb(aos, f, make_geo(N), st);
+}
 
-cudaError_t launch_rb_to_aos(Fields f, double *aos, int N, cudaStream_t st) {
-  const Geo g = make_geo(N);
+cudaError_t launch_rb_to_aos(Fields f, double *aos, const Geo &g, cudaStream_t st) {
   rb_to_aos_kernel<<<nblocks(2 * g.V2, kThreads), kThreads, 0, st>>>(f, aos, g);
   return cudaGetLastError();
+}
+cudaError_t launch_rb_to_aos(Fields f, double *aos, int N, cudaStream_t st) {
+  return launch_rb_to_aos(f, aos, make_geo(N), st);
 }
 
 cudaError_t launch_init_phi(Fields f, int N, uint64_t sk, double scale, cudaStream_t st) {
@@ -2370,7 +2375,10 @@ cudaError_t launch_hb_zpass(Fields f, int N, int parity, const HbArgs &a, cudaSt
 
 cudaError_t launch_hb_pass(Fields f, int N, int parity, const HbArgs &a, cudaStream_t st) {
   if (hb_zpass_default(N)) return launch_hb_zpass(f, N, parity, a, st);
-  const Geo g = make_geo(N);
+  return launch_hb_pass(f, make_geo(N), parity, a, st);
+}
+
+cudaError_t launch_hb_pass(Fields f, const Geo &g, int parity, const HbArgs &a, cudaStream_t st) {
   const bool rows = g.H % 128 == 0;
   const dim3 grid = pass_grid(g, rows);
   const bool inj = a.prop != nullptr, mon = a.mon != nullptr;
@@ -2532,7 +2540,10 @@ cudaError_t launch_hb_sweep(Fields in, Fields out, int N, const HbArgs &a, cudaS
 }
 
 cudaError_t launch_charge_pass(Fields f, int N, int dir, int eoA, const ChargeArgs &a, cudaStream_t st) {
-  const Geo g = make_geo(N);
+  return launch_charge_pass(f, make_geo(N), dir, eoA, a, st);
+}
+
+cudaError_t launch_charge_pass(Fields f, const Geo &g, int dir, int eoA, const ChargeArgs &a, cudaStream_t st) {
   const bool rows = g.H % 128 == 0;
   const dim3 grid = pass_grid(g, rows);
   const bool inj = a.q != nullptr, mon = a.mon != nullptr;
@@ -2645,7 +2656,10 @@ cudaError_t launch_charge_dir(Fields in, Fields out, int N, int dir, const Charg
 }
 
 cudaError_t launch_em(Fields in, Fields out, int N, const EmArgs &a, cudaStream_t st) {
-  const Geo g = make_geo(N);
+  return launch_em(in, out, make_geo(N), a, st);
+}
+
+cudaError_t launch_em(Fields in, Fields out, const Geo &g, const EmArgs &a, cudaStream_t st) {
   const unsigned nb = nblocks(g.V2, kThreads);
   if (a.xi) em_kernel<true, false><<<nb, kThreads, 0, st>>>(in, out, g, a, nullptr, nullptr, nullptr);
   else em_kernel<false, false><<<nb, kThreads, 0, st>>>(in, out, g, a, nullptr, nullptr, nullptr);
@@ -2662,20 +2676,24 @@ cudaError_t launch_em_avg(Fields in, Fields out, int N, const EmArgs &a, double 
 }
 
 cudaError_t launch_ideal(Fields in, Fields out, int N, const IdealArgs &a, cudaStream_t st) {
-  const Geo g = make_geo(N);
+  return launch_ideal(in, out, make_geo(N), a, st);
+}
+
+cudaError_t launch_ideal(Fields in, Fields out, const Geo &g, const IdealArgs &a, cudaStream_t st) {
+  const int N = g.N;
   constexpr int TX = 32, TY = 8;
   using T = IdealTile<TX, TY>;
   const long long bxy = (long long)((N + TX - 1) / TX) * ((N + TY - 1) / TY);
-  long long zc = (long long)N * bxy / 1184;
+  long long zc = (long long)g.Nz * bxy / 1184;
   if (zc > 32) zc = 32;
   if (zc < 4) zc = 4;
-  if (zc > N) zc = N;
+  if (zc > g.Nz) zc = g.Nz;
   static const bool tma_off = [] {
     const char *v = std::getenv("LGV_IDEAL_TMA");
     return v && v[0] == '0';
   }();
-  if (!tma_off && ideal_tma_supported(N)) return launch_ideal_tma(in, out, N, (int)zc, a, st);
-  dim3 grid((N + TX - 1) / TX, (N + TY - 1) / TY, (unsigned)((N + zc - 1) / zc));
+  if (!tma_off && ideal_tma_supported(N)) return launch_ideal_tma(in, out, g, (int)zc, a, st);
+  dim3 grid((N + TX - 1) / TX, (N + TY - 1) / TY, (unsigned)((g.Nz + zc - 1) / zc));
   cudaError_t e = allow_smem(ideal_kernel<TX, TY>, T::SMEM);
   if (e != cudaSuccess) return e;
   ideal_kernel<TX, TY><<<grid, TX * TY, T::SMEM, st>>>(in, out, g, (int)zc, a);
@@ -2707,8 +2725,8 @@ cudaError_t launch_measure(Fields f, int N, double *scratch, double *dev_out, cu
   const Geo g = make_geo(N);
   const long long NN = (long long)N * N;
   double *T = scratch, *U = scratch + (size_t)kNObs * NN;
-  meas_sum_j_kernel<<<nblocks(NN, 128), 128, 0, st>>>(f, g, T);
-  meas_sum_k_kernel<<<nblocks(NN, 128), 128, 0, st>>>(f, g, U);
+  meas_sum_j_kernel<<<nblocks(NN, 128), 128, 0, st>>>(f, g, T, 0, N, 0);
+  meas_sum_k_kernel<<<nblocks(NN, 128), 128, 0, st>>>(f, g, U, 0, N);
   const MeasOut mo = meas_layout(dev_out, N);
   meas_walls_kernel<<<nblocks(3LL * kNObs * N, 128), 128, 0, st>>>(T, U, N, mo);
   const int NK = N / 2 + 1;
@@ -2717,6 +2735,14 @@ cudaError_t launch_measure(Fields f, int N, double *scratch, double *dev_out, cu
   return cudaGetLastError();
 }
 
+
+cudaError_t launch_measure_partials(Fields f, const Geo &g, int klo, int nk, int kout, double *T, double *U,
+                                    cudaStream_t st) {
+  const long long NN = (long long)g.N * g.N;
+  meas_sum_j_kernel<<<nblocks((long long)g.N * nk, 128), 128, 0, st>>>(f, g, T, klo, nk, kout);
+  meas_sum_k_kernel<<<nblocks(NN, 128), 128, 0, st>>>(f, g, U, klo, nk);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_measure_sums_aos(const double *aos, int N, double *T, double *U, cudaStream_t st) {
   const long long NN = (long long)N * N;
