@@ -322,6 +322,74 @@ MODEL_G_64 = dict(N=64, steps=10000, measure_every=10, mass0=-4.813, lam=10.0, H
                   diffusion=1.0 / 3.0, dt=0.04)
 
 
+def run_slab_emulated(N=256, R=2, steps=5):
+    """The z-slab decomposition on one GPU: R slabs of the N^3 lattice, each
+    stepping in its own host thread, ghost planes refreshed by device copies
+    at host barriers before every cross-plane sub-pass (ThreadHalo).  Reports
+    the PV2HBSplit23 step time of the split lattice (wall clock around the
+    threads; all slabs share the GPU) against one whole-lattice handle, and the
+    exchanges per step.  On one GPU this measures the cost of the exchanges
+    and their host synchronisation, not multi-GPU scaling."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from langevina_b200 import _lib as L
+    from langevina_b200 import slab as S
+
+    rng = np.random.default_rng(5)
+    u = np.zeros((N, N, N, 10))
+    u[..., :4] = 0.1 * rng.normal(size=(N, N, N, 4))
+    u[..., 4:] = np.sqrt(COEF["chi"]) * rng.normal(size=(N, N, N, 6))
+    halo = S.ThreadHalo(R)
+    calls = [0]
+    inner_exchange = halo.exchange
+
+    def counted(slab, comps):
+        if slab.rank == 0:
+            calls[0] += 1
+        inner_exchange(slab, comps)
+
+    halo.exchange = counted
+    slabs = [S.SlabLattice(N, k0, nz, halo, rank=r, seed=99, **COEF) for r, (k0, nz) in enumerate(S.slab_planes(N, R))]
+    try:
+        for s_ in slabs:
+            halo.attach(s_)
+            s_.set_global_state(u)
+        S.run_threads(slabs, lambda s_: s_.step(L.PV2HBSPLIT, DT, inner=2, outer=3, nsteps=1))
+        calls[0] = 0
+        t0 = time.perf_counter()
+        S.run_threads(slabs, lambda s_: s_.step(L.PV2HBSPLIT, DT, inner=2, outer=3, nsteps=steps))
+        for s_ in slabs:
+            s_.sync()
+        ms_split = (time.perf_counter() - t0) / steps * 1e3
+        exchanges = calls[0] / steps
+    finally:
+        for s_ in slabs:
+            s_.close()
+    lib = L.load()
+    p = L.make_params(N, seed=99, **COEF)
+    h = C.c_void_p()
+    L.check(lib.lgv_create(C.byref(p), C.byref(h)), "create")
+    try:
+        L.check(lib.lgv_set_state(h, L.ptr(np.ascontiguousarray(u))), "set_state")
+        L.check(lib.lgv_step(h, L.PV2HBSPLIT, 2, 3, DT, 0.0, 1), "warm")
+        L.check(lib.lgv_synchronize(h), "sync")
+        t0 = time.perf_counter()
+        L.check(lib.lgv_step(h, L.PV2HBSPLIT, 2, 3, DT, 0.0, steps), "step")
+        L.check(lib.lgv_synchronize(h), "sync")
+        ms_whole = (time.perf_counter() - t0) / steps * 1e3
+    finally:
+        lib.lgv_destroy(h)
+    torch.cuda.synchronize()
+    return {"workload": f"PV2HBSplit23 on {N}^3 split into {R} z-slabs emulated on one GPU (host threads, "
+                        f"device copies of the ghost planes at host barriers)",
+            "ranks": R, "split_ms_per_step": ms_split, "whole_ms_per_step": ms_whole,
+            "split_over_whole": ms_split / ms_whole, "exchanges_per_step": exchanges,
+            "timing": "host wall clock around the steps (both arms), after one warm-up step"}
+
+
 def run_model_g_64():
     """Full Model G on 64^3 with the (1, 1) composer (one ideal step, one phi
     heat-bath sweep, one charge heat bath per step), charges starting at 0, phi
@@ -810,8 +878,10 @@ def run_ours(a):
         adjoint = run_adjoint()
         adjoint["batched"] = run_adjoint_batch()
     model_g_64 = None
+    slab = None
     if world == 1 and not a.no_variants:
         model_g_64 = run_model_g_64()
+        slab = run_slab_emulated()
     postprocess = None
     if world == 1 and not a.no_postprocess:
         postprocess = run_postprocess()
@@ -837,6 +907,7 @@ def run_ours(a):
         "adjoint": adjoint,
         "variants": variants,
         "model_g_64cubed": model_g_64,
+        "slab_emulated": slab,
         "postprocess": postprocess,
         "gpu_launches": launches,
         "clocks": ck,

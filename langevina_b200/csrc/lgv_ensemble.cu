@@ -80,6 +80,13 @@ struct lgv_ensemble {
   // and the polls before one gives up (LGV_WAIT_LIMIT at creation)
   unsigned long long *waits = nullptr;
   int wait_limit = lgv::kWaitLimit;
+  // The ideal step's two launches (TMA replicas, cp.async replicas) write
+  // disjoint replicas: the cp.async one runs on `side`, forked from and joined
+  // back into `stream` by events (also inside graph capture), so the two
+  // overlap.  LGV_ENS_CONCURRENT=0 at creation keeps them in sequence.
+  bool concurrent = true;
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
   // differentiable Euler-Maruyama run (lgv_ensemble_diff_forward / _backward)
   struct {
     bool ready = false;
@@ -252,12 +259,21 @@ int enqueue_step(lgv_ensemble *e, int ev, int inner, int outer, double dt) {
   const int nb_i = e->ideal_map.nblocks, nb_p = e->plane_map.nblocks, nb_s = e->slab_map.nblocks;
   int off = 0;
   auto ideal = [&](double d) -> int {
+    const bool both = e->concurrent && e->side && e->tma_map.nblocks > 0 && nb_i > 0;
+    if (both) {
+      ECK(cudaEventRecord(e->fork, e->stream));
+      ECK(cudaStreamWaitEvent(e->side, e->fork, 0));
+    }
     if (e->tma_map.nblocks > 0)
       ECK(lgv::launch_batch_ideal_tma(e->dd, e->gmaps, e->tma_map.rep, e->tma_map.first, e->tma_map.nblocks,
                                       e->phase_phi, e->phase_q, d, e->waits, e->wait_limit, e->stream));
     if (nb_i > 0)
       ECK(lgv::launch_batch_ideal(e->dd, e->ideal_map.rep, e->ideal_map.first, nb_i, e->tile, e->phase_phi,
-                                  e->phase_q, d, e->stream));
+                                  e->phase_q, d, both ? e->side : e->stream));
+    if (both) {
+      ECK(cudaEventRecord(e->join, e->side));
+      ECK(cudaStreamWaitEvent(e->stream, e->join, 0));
+    }
     // the ideal step writes all ten components to the other buffer
     e->phase_phi ^= 1;
     e->phase_q ^= 1;
@@ -348,6 +364,14 @@ int lgv_ensemble_create(int nrep, const lgv_params *params, lgv_ensemble **out) 
   if (cudaMalloc((void **)&e->waits, sizeof(unsigned long long)) != cudaSuccess ||
       cudaMemset(e->waits, 0, sizeof(unsigned long long)) != cudaSuccess)
     return bail(efail(LGV_ERR_NOMEM, "wait counter"));
+  {
+    const char *cv = std::getenv("LGV_ENS_CONCURRENT");
+    e->concurrent = !(cv && cv[0] == '0');
+  }
+  if (cudaStreamCreateWithFlags(&e->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&e->join, cudaEventDisableTiming) != cudaSuccess)
+    return bail(efail(LGV_ERR_CUDA, "side stream"));
   e->hd.resize(nrep);
   for (int r = 0; r < nrep; ++r) {
     const lgv_params &q = params[r];
@@ -406,6 +430,12 @@ int lgv_ensemble_destroy(lgv_ensemble *e) {
   if (e->diff.partial) cudaFree(e->diff.partial);
   if (e->diff.done) cudaFree(e->diff.done);
   if (e->waits) cudaFree(e->waits);
+  if (e->side) {
+    cudaStreamSynchronize(e->side);
+    cudaStreamDestroy(e->side);
+  }
+  if (e->fork) cudaEventDestroy(e->fork);
+  if (e->join) cudaEventDestroy(e->join);
   if (e->own) cudaStreamDestroy(e->own);
   delete e;
   return LGV_OK;
