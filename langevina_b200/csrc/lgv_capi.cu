@@ -106,6 +106,12 @@ struct lgv_handle {
   // lgv_create; the default is lgv::kWaitLimit)
   unsigned long long *waits_dev = nullptr;
   int wait_limit = lgv::kWaitLimit;
+  // Plane order of the next ideal, phi-pass or charge-face launch: it flips
+  // after every such launch, so each pass starts on the planes the previous
+  // one touched last (still in L2).  LGV_ZALT=0 at creation keeps every pass
+  // bottom-up.
+  bool zalt = true;
+  int zrev = 0;
   // Geometry of the buffers: the whole lattice, or for a slab handle
   // (lgv_slab_create) its planes k0 .. k0+nz-1 with two ghost planes on each
   // side, filled by the caller's halo exchange before every sub-pass that
@@ -271,6 +277,16 @@ int energy_now(lgv_handle *h, double *E) {
 }
 
 // --- sub-steps -------------------------------------------------------------
+// Geometry for the next pass launch, in the plane order its turn gives.
+lgv::Geo pass_geo(lgv_handle *h) {
+  lgv::Geo g = h->geo;
+  if (h->zalt) {
+    g.zrev = h->zrev;
+    h->zrev ^= 1;
+  }
+  return g;
+}
+
 int sub_ideal(lgv_handle *h, double dt) {  // IdealPV2::step (Stepper.cxx:23-66)
   double Eold = 0, Enew = 0;
   if (h->mon_on) LGV_TRY(energy_now(h, &Eold));
@@ -285,7 +301,7 @@ int sub_ideal(lgv_handle *h, double dt) {  // IdealPV2::step (Stepper.cxx:23-66)
   LGV_TRY(halo(h, LGV_HALO_ALL));
   {
     KTimer tm(h, LGV_KCLASS_IDEAL);
-    LGV_CK(lgv::launch_ideal(h->cur, h->alt, h->geo, a, h->stream));
+    LGV_CK(lgv::launch_ideal(h->cur, h->alt, pass_geo(h), a, h->stream));
   }
   std::swap(h->cur, h->alt);
   if (h->mon_on) {
@@ -329,8 +345,7 @@ int sub_hb(lgv_handle *h, double dt, double mass) {  // EulerLangevinHB::step (S
     for (int parity = 0; parity < 2; ++parity) {
       LGV_TRY(halo(h, LGV_HALO_PHI));
       KTimer tm(h, LGV_KCLASS_PHI_HB);
-      if (h->slab) LGV_CK(lgv::launch_hb_pass(h->cur, h->geo, parity, a, h->stream));
-      else LGV_CK(lgv::launch_hb_pass(h->cur, h->N, parity, a, h->stream));
+      LGV_CK(lgv::launch_hb_pass(h->cur, pass_geo(h), parity, a, h->stream));
     }
   }
   if (h->noise_mode == LGV_NOISE_INJECTED) h->have_hb = false;
@@ -399,7 +414,7 @@ int sub_charge(lgv_handle *h, double dt) {  // ModelGChargeHB::step (Stepper.cxx
       if (h->noise_mode != LGV_NOISE_INJECTED) a.sk = lgv::sub_key(h->key, h->ctr + 1 + p);
       if (xyz[p / 2] == 2) LGV_TRY(halo(h, LGV_HALO_CHARGES));  // links across planes
       KTimer tm(h, LGV_KCLASS_CHARGE);
-      LGV_CK(lgv::launch_charge_pass(h->cur, h->geo, xyz[p / 2], eo[p % 2], a, h->stream));
+      LGV_CK(lgv::launch_charge_pass(h->cur, pass_geo(h), xyz[p / 2], eo[p % 2], a, h->stream));
     }
   } else {
     // both faces of a direction per launch (same streams and order as per face)
@@ -546,6 +561,8 @@ int create_handle(const lgv_params *params, const lgv::Geo &g, bool slab, int k0
   {
     const char *wl = std::getenv("LGV_WAIT_LIMIT");
     if (wl && wl[0]) h->wait_limit = std::max(0, std::atoi(wl));
+    const char *za = std::getenv("LGV_ZALT");
+    h->zalt = !(za && za[0] == '0');
   }
   int rc = LGV_OK;
   if (cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess) {

@@ -31,6 +31,11 @@ struct Geo {
   int Nz;        // planes in the buffer
   int kg;        // global plane of local plane 0 (0 for a whole lattice)
   int Ng;        // planes of the whole lattice (N)
+  // 1: the blocks of a pass take the planes (or z-chunks) from the top down.
+  // Every pass is independent of the order its sites are visited in, so
+  // consecutive passes alternate the order and each starts on the planes the
+  // previous one left in L2.
+  int zrev;
 };
 
 __host__ __device__ __forceinline__ Geo make_geo(int N) {
@@ -41,6 +46,7 @@ __host__ __device__ __forceinline__ Geo make_geo(int N) {
   g.Nz = N;
   g.kg = 0;
   g.Ng = N;
+  g.zrev = 0;
   return g;
 }
 

@@ -143,11 +143,23 @@ __device__ __forceinline__ void ideal_tma_cta(const CUtensorMap *maps, const Fie
   // Plane q of the march (q = 0 is z0-1, which feeds only the own column's
   // z-1 neighbour and needs no ring) goes to stage q % NS; one cp.async group
   // per plane, possibly empty, so waiting for all groups covers plane q.
+  // Planes are tracked incrementally (q covers z0-1 .. z1, within one wrap of
+  // the buffer), so the march does no integer division.
+  const int zfirst = z0 == 0 ? g.Nz - 1 : z0 - 1;  // plane of q = 0
+  const long long NH = (long long)N * g.H;
+  const int ring_xy = hyg * g.H + (hxg >> 1);  // in-plane parts of the ring and own sites' offsets
+  const int own_xy = yj * g.H + (xi >> 1);
+  auto plane_of = [&](int q) {  // zfirst + q wrapped; q < nit <= Nz + 2, so at most two wraps
+    int pl = zfirst + q;
+    if (pl >= g.Nz) pl -= g.Nz;
+    if (pl >= g.Nz) pl -= g.Nz;
+    return pl;
+  };
   auto issue = [&](int q) {
-    const int pl = wrapn(z0 - 1 + q, g.Nz), sn = q % NS;
+    const int pl = plane_of(q), sn = q % NS;
     if (tid == 0) issue_plane(maps, core + sn * 10 * CORE, bar0 + 8 * sn, x0 / 2, y0, pl);
     if (ring && q >= 1) {
-      const long long oh = rb_off(g, hxg, hyg, pl);
+      const long long oh = (long long)((hxg + hyg + pl) & 1) * g.V2 + (long long)pl * NH + ring_xy;
 #pragma unroll
       for (int c = 0; c < 10; ++c) cp_async8(&halo[(sn * 10 + c) * NHALO + tid], in.c[c] + oh);
     }
@@ -159,8 +171,9 @@ __device__ __forceinline__ void ideal_tma_cta(const CUtensorMap *maps, const Fie
 
   double pm[4], pc[4], pn[4], qc[6], qn[6];
   unsigned wbar = bar0, wpar = 0;  // the barrier phase waited on last
+  int kk = zfirst;  // plane p - 1 (used from it >= 2)
   for (int it = 0; it < nit; ++it) {
-    const int p = wrapn(z0 - 1 + it, g.Nz);
+    const int p = plane_of(it);
     const int st = it % NS;
     wbar = bar0 + 8 * st;
     wpar = (unsigned)((it / NS) & 1);
@@ -203,7 +216,6 @@ __device__ __forceinline__ void ideal_tma_cta(const CUtensorMap *maps, const Fie
       // phi' of plane p-1, written last iteration; the barrier at the top of
       // this iteration also ends last iteration's reads of the buffer written now
       const double *pp = phs + ((it + 1) & 1) * 4 * PH;
-      const int kk = wrapn(p - 1, g.Nz);
       const int nh = ((hw + y0 + ty + kk) & 1) ^ 1;  // the neighbours' half
       const int rx = (nh * PR + ty + 1) * PM;
       const int oxp = rx + t + 1 + hw, oxm = rx + t + hw;
@@ -224,7 +236,7 @@ __device__ __forceinline__ void ideal_tma_cta(const CUtensorMap *maps, const Fie
       // second half rotation on a copy: pc (phi') stays the z-1 neighbour of the next plane
       double pf[4] = {pc[0], pc[1], pc[2], pc[3]};
       rotate_site(pf, qc, a.dto2chi);
-      const long long o = rb_off(g, xi, yj, kk);
+      const long long o = (long long)((xi + yj + kk) & 1) * g.V2 + (long long)kk * NH + own_xy;
 #pragma unroll
       for (int l = 0; l < 4; ++l) out.c[l][o] = pf[l];
 #pragma unroll
@@ -237,6 +249,7 @@ __device__ __forceinline__ void ideal_tma_cta(const CUtensorMap *maps, const Fie
     }
 #pragma unroll
     for (int s = 0; s < 6; ++s) qc[s] = qn[s];
+    kk = p;
   }
   if (s_abort) {
     // the plane that timed out may still be in flight: one more bounded wait
@@ -249,7 +262,8 @@ __device__ __forceinline__ void ideal_tma_cta(const CUtensorMap *maps, const Fie
 
 __global__ void __launch_bounds__(NT, 2)
     ideal_tma_kernel(const __grid_constant__ TmaMaps maps, Fields in, Fields out, Geo g, int zchunk, IdealArgs a) {
-  ideal_tma_cta(maps.m, in, out, g, zchunk, a, blockIdx.x, blockIdx.y, blockIdx.z);
+  ideal_tma_cta(maps.m, in, out, g, zchunk, a, blockIdx.x, blockIdx.y,
+                g.zrev ? (int)(gridDim.z - 1 - blockIdx.z) : (int)blockIdx.z);
 }
 
 // Ensembles: the CTAs of every replica with N divisible by 32 in one launch,

@@ -319,7 +319,22 @@ __device__ __forceinline__ double ld_phi(const double *p) {
   return *p;
 }
 
-template <bool INJECTED, bool MON, bool CG = false>
+// I: the type of element offsets -- int when the buffer (2 V2 elements) and
+// the lattice's global site count fit in 31 bits (idx32), so that every load
+// address is one wide multiply-add of a component base; long long otherwise.
+__host__ __forceinline__ bool idx32(const Geo &g) {
+  return 2 * g.V2 <= 0x7fffffffLL && (long long)g.N * g.N * g.Ng <= 0x7fffffffLL;
+}
+
+template <typename I>
+__device__ __forceinline__ I nat_index_t(const Geo &g, int i, int j, int k) {
+  int kk = k + g.kg;
+  if (kk < 0) kk += g.Ng;
+  else if (kk >= g.Ng) kk -= g.Ng;
+  return ((I)kk * g.N + j) * g.N + i;
+}
+
+template <bool INJECTED, bool MON, bool CG = false, typename I = long long>
 __device__ __forceinline__ void hb_site(const Fields &f, const Geo &g, int parity, const HbArgs &a, int m, int j,
                                         int k, MonLocal &mon) {
   const int H = g.H, N = g.N;
@@ -327,23 +342,24 @@ __device__ __forceinline__ void hb_site(const Fields &f, const Geo &g, int parit
   int xm = m - 1 + s, xp = m + s;
   if (xm < 0) xm += H;
   if (xp == H) xp = 0;
-  const long long row = ((long long)k * N + j) * H;
-  const long long rjp = ((long long)k * N + wrap_inc(j, N)) * H;
-  const long long rjm = ((long long)k * N + wrap_dec(j, N)) * H;
-  const long long rkp = ((long long)wrap_inc(k, g.Nz) * N + j) * H;
-  const long long rkm = ((long long)wrap_dec(k, g.Nz) * N + j) * H;
-  const long long own = (long long)parity * g.V2 + row + m;
-  const long long ob = (long long)(parity ^ 1) * g.V2;
+  const I ob = (I)(parity ^ 1) * (I)g.V2;
+  const I row = ((I)k * N + j) * H;
+  const I orow = ob + row;
+  const I ojp = ob + ((I)k * N + wrap_inc(j, N)) * H + m;
+  const I ojm = ob + ((I)k * N + wrap_dec(j, N)) * H + m;
+  const I okp = ob + ((I)wrap_inc(k, g.Nz) * N + j) * H + m;
+  const I okm = ob + ((I)wrap_dec(k, g.Nz) * N + j) * H + m;
+  const I own = (I)parity * (I)g.V2 + row + m;
   double po[4], heff[4];
 #pragma unroll
   for (int l = 0; l < 4; ++l) {
     const double *P = f.c[l];
-    heff[l] = (ld_phi<CG>(P + ob + row + xp) + ld_phi<CG>(P + ob + row + xm)) +
-              (ld_phi<CG>(P + ob + rjp + m) + ld_phi<CG>(P + ob + rjm + m)) +
-              (ld_phi<CG>(P + ob + rkp + m) + ld_phi<CG>(P + ob + rkm + m));
+    heff[l] = (ld_phi<CG>(P + (orow + xp)) + ld_phi<CG>(P + (orow + xm))) +
+              (ld_phi<CG>(P + ojp) + ld_phi<CG>(P + ojm)) +
+              (ld_phi<CG>(P + okp) + ld_phi<CG>(P + okm));
     po[l] = ld_phi<CG>(P + own);
   }
-  const long long nat = nat_index(g, 2 * m + s, j, k);
+  const long long nat = (long long)nat_index_t<I>(g, 2 * m + s, j, k);
   HbDecision d;
   hb_decide<INJECTED>(po, heff, a, nat, global_sites(g), d);
   if (d.accept) {
@@ -363,7 +379,7 @@ __device__ __forceinline__ bool pass_site(const Geo &g, int &m, int &j, int &k) 
   if (ROWS) {
     m = blockIdx.x * 128 + threadIdx.x;
     j = blockIdx.y;
-    k = blockIdx.z;
+    k = g.zrev ? (int)(gridDim.z - 1 - blockIdx.z) : (int)blockIdx.z;
     return true;
   }
   const unsigned t = blockIdx.x * 128 + threadIdx.x, H = (unsigned)g.H;
@@ -371,7 +387,7 @@ __device__ __forceinline__ bool pass_site(const Geo &g, int &m, int &j, int &k) 
   const unsigned jj = t / H;
   m = (int)(t - jj * H);
   j = (int)jj;
-  k = blockIdx.y;
+  k = g.zrev ? (int)(gridDim.y - 1 - blockIdx.y) : (int)blockIdx.y;
   return true;
 }
 
@@ -379,11 +395,11 @@ __host__ __forceinline__ dim3 pass_grid(const Geo &g, bool rows) {
   return rows ? dim3(g.H / 128, g.N, g.Nz) : dim3((unsigned)(((long long)g.N * g.H + 127) / 128), g.Nz);
 }
 
-template <bool INJECTED, bool MON, bool ROWS>
+template <bool INJECTED, bool MON, bool ROWS, typename I>
 __global__ void __launch_bounds__(128) hb_pass_kernel(Fields f, Geo g, int parity, HbArgs a) {
   int m, j, k;
   MonLocal mon;
-  if (pass_site<ROWS>(g, m, j, k)) hb_site<INJECTED, MON>(f, g, parity, a, m, j, k, mon);
+  if (pass_site<ROWS>(g, m, j, k)) hb_site<INJECTED, MON, false, I>(f, g, parity, a, m, j, k, mon);
   if (MON) mon_flush(mon, a.mon);
 }
 
@@ -771,25 +787,25 @@ __global__ void __launch_bounds__(HB_TM *HB_TY, 2) hb_sweep_kernel(Fields in, Fi
 // Charge heat bath, one face (direction `dir`, A-site parity eoA).  One thread
 // per link (A, B = A + e_dir); the links of a face are disjoint, so the update
 // is race free and conserves each charge exactly (Stepper.cxx:493-517).
-template <bool INJECTED, bool MON>
+template <bool INJECTED, bool MON, typename I = long long>
 __device__ __forceinline__ void charge_link_site(const Fields &f, const Geo &g, int dir, int eoA, const ChargeArgs &a,
                                                  int m, int j, int k, MonLocal &mon) {
   const int H = g.H, N = g.N;
   const int s = (eoA + j + k) & 1;
   const int i = 2 * m + s;
-  const long long offA = (long long)eoA * g.V2 + ((long long)k * N + j) * H + m;
-  long long offB;
-  const long long ob = (long long)(eoA ^ 1) * g.V2;
+  const I offA = (I)eoA * (I)g.V2 + ((I)k * N + j) * H + m;
+  I offB;
+  const I ob = (I)(eoA ^ 1) * (I)g.V2;
   if (dir == 0) {
     int mb = m + s;
     if (mb == H) mb = 0;
-    offB = ob + ((long long)k * N + j) * H + mb;
+    offB = ob + ((I)k * N + j) * H + mb;
   } else if (dir == 1) {
-    offB = ob + ((long long)k * N + wrap_inc(j, N)) * H + m;
+    offB = ob + ((I)k * N + wrap_inc(j, N)) * H + m;
   } else {
-    offB = ob + ((long long)wrap_inc(k, g.Nz) * N + j) * H + m;
+    offB = ob + ((I)wrap_inc(k, g.Nz) * N + j) * H + m;
   }
-  const long long nat = nat_index(g, i, j, k);
+  const long long nat = (long long)nat_index_t<I>(g, i, j, k);
   const long long V = global_sites(g);
   WordStream ws{};
   if (!INJECTED) ws = words_at(a.sk, 6 * (uint64_t)nat);
@@ -835,11 +851,11 @@ __device__ __forceinline__ void charge_link_site(const Fields &f, const Geo &g, 
 // Grid as hb_pass_kernel (pass_site).
 // 16 blocks of 128 threads per SM (32 registers): the link updates are long
 // integer / FP64 chains, and full occupancy hides them best
-template <bool INJECTED, bool MON, bool ROWS>
+template <bool INJECTED, bool MON, bool ROWS, typename I>
 __global__ void __launch_bounds__(128, 16) charge_pass_kernel(Fields f, Geo g, int dir, int eoA, ChargeArgs a) {
   int m, j, k;
   MonLocal mon;
-  if (pass_site<ROWS>(g, m, j, k)) charge_link_site<INJECTED, MON>(f, g, dir, eoA, a, m, j, k, mon);
+  if (pass_site<ROWS>(g, m, j, k)) charge_link_site<INJECTED, MON, I>(f, g, dir, eoA, a, m, j, k, mon);
   if (MON) mon_flush(mon, a.mon);
 }
 
@@ -1435,7 +1451,8 @@ __device__ __forceinline__ void ideal_tile(const Fields &in, const Fields &out, 
 
 template <int TX, int TY>
 __global__ void __launch_bounds__(TX *TY, 2) ideal_kernel(Fields in, Fields out, Geo g, int zchunk, IdealArgs a) {
-  ideal_tile<TX, TY>(in, out, g, zchunk, a, blockIdx.x, blockIdx.y, blockIdx.z);
+  ideal_tile<TX, TY>(in, out, g, zchunk, a, blockIdx.x, blockIdx.y,
+                    g.zrev ? (int)(gridDim.z - 1 - blockIdx.z) : (int)blockIdx.z);
 }
 
 // ----------------------------------------------------------------------------
@@ -2379,15 +2396,20 @@ cudaError_t launch_hb_pass(Fields f, int N, int parity, const HbArgs &a, cudaStr
 }
 
 cudaError_t launch_hb_pass(Fields f, const Geo &g, int parity, const HbArgs &a, cudaStream_t st) {
+  if (g.Nz == g.Ng && g.kg == 0 && hb_zpass_default(g.N)) return launch_hb_zpass(f, g.N, parity, a, st);
   const bool rows = g.H % 128 == 0;
   const dim3 grid = pass_grid(g, rows);
   const bool inj = a.prop != nullptr, mon = a.mon != nullptr;
+  const bool i32 = idx32(g);
+#define LGV_HBP1(I, M, T)                                                                                    \
+  if (rows) hb_pass_kernel<I, M, true, T><<<grid, 128, 0, st>>>(f, g, parity, a);                           \
+  else hb_pass_kernel<I, M, false, T><<<grid, 128, 0, st>>>(f, g, parity, a)
 #define LGV_HBP(I, M)                                                                                        \
-  if (rows) hb_pass_kernel<I, M, true><<<grid, 128, 0, st>>>(f, g, parity, a);                              \
-  else hb_pass_kernel<I, M, false><<<grid, 128, 0, st>>>(f, g, parity, a)
+  if (i32) { LGV_HBP1(I, M, int); } else { LGV_HBP1(I, M, long long); }
   if (inj) { if (mon) { LGV_HBP(true, true); } else { LGV_HBP(true, false); } }
   else { if (mon) { LGV_HBP(false, true); } else { LGV_HBP(false, false); } }
 #undef LGV_HBP
+#undef LGV_HBP1
   return cudaGetLastError();
 }
 
@@ -2547,12 +2569,16 @@ cudaError_t launch_charge_pass(Fields f, const Geo &g, int dir, int eoA, const C
   const bool rows = g.H % 128 == 0;
   const dim3 grid = pass_grid(g, rows);
   const bool inj = a.q != nullptr, mon = a.mon != nullptr;
+  const bool i32 = idx32(g);
+#define LGV_CHP1(I, M, T)                                                                                    \
+  if (rows) charge_pass_kernel<I, M, true, T><<<grid, 128, 0, st>>>(f, g, dir, eoA, a);                     \
+  else charge_pass_kernel<I, M, false, T><<<grid, 128, 0, st>>>(f, g, dir, eoA, a)
 #define LGV_CHP(I, M)                                                                                        \
-  if (rows) charge_pass_kernel<I, M, true><<<grid, 128, 0, st>>>(f, g, dir, eoA, a);                        \
-  else charge_pass_kernel<I, M, false><<<grid, 128, 0, st>>>(f, g, dir, eoA, a)
+  if (i32) { LGV_CHP1(I, M, int); } else { LGV_CHP1(I, M, long long); }
   if (inj) { if (mon) { LGV_CHP(true, true); } else { LGV_CHP(true, false); } }
   else { if (mon) { LGV_CHP(false, true); } else { LGV_CHP(false, false); } }
 #undef LGV_CHP
+#undef LGV_CHP1
   return cudaGetLastError();
 }
 
