@@ -86,6 +86,8 @@ struct lgv_ensemble {
   // overlap.  LGV_ENS_CONCURRENT=0 at creation keeps them in sequence.
   bool concurrent = true;
   cudaStream_t side = nullptr;
+  // every replica's element offsets fit 31 bits (set at creation)
+  bool idx32 = false;
   cudaEvent_t fork = nullptr, join = nullptr;
   // differentiable Euler-Maruyama run (lgv_ensemble_diff_forward / _backward)
   struct {
@@ -282,14 +284,14 @@ int enqueue_step(lgv_ensemble *e, int ev, int inner, int outer, double dt) {
   auto hb = [&](double d) -> int {
     for (int parity = 0; parity < 2; ++parity)
       ECK(lgv::launch_batch_hb(e->dd, e->dyn, e->slab_map.rep, e->slab_map.first, nb_s, e->phase_phi, parity, d, off,
-                               e->stream));
+                               e->idx32, e->stream));
     off += 1;
     return LGV_OK;
   };
   auto charge = [&](double d) -> int {
     for (int pass = 0; pass < 6; ++pass)
       ECK(lgv::launch_batch_charge(e->dd, e->dyn, e->slab_map.rep, e->slab_map.first, nb_s, e->phase_q, pass, d,
-                                   off, e->stream));
+                                   off, e->idx32, e->stream));
     off += 7;
     return LGV_OK;
   };
@@ -397,6 +399,7 @@ int lgv_ensemble_create(int nrep, const lgv_params *params, lgv_ensemble **out) 
       d.base[b] = buf;
     }
   }
+  e->idx32 = lgv::batch_idx32(e->hd.data(), nrep);
   if (cudaMalloc((void **)&e->dd, nrep * sizeof(RepDesc)) != cudaSuccess ||
       cudaMalloc((void **)&e->dyn, sizeof(EnsDyn)) != cudaSuccess ||
       cudaMalloc((void **)&e->oavg, (size_t)nrep * 11 * sizeof(double)) != cudaSuccess)

@@ -130,10 +130,13 @@ constexpr int kBatchPlanes = 4;
 cudaError_t launch_batch_ideal(const RepDesc *d, const int *rep, const int *first, int nblocks, int tile,
                                int phase_phi, int phase_q, double dt, cudaStream_t st);
 // rep / first / nblocks of launch_batch_hb and launch_batch_charge: the slab map (kBatchPlanes planes per block)
+// true when every replica's element offsets fit 31 bits (the batched heat-bath
+// and charge kernels then index with int; i32 of their launchers)
+bool batch_idx32(const RepDesc *hd, int nrep);
 cudaError_t launch_batch_hb(const RepDesc *d, const EnsDyn *dyn, const int *rep, const int *first, int nblocks,
-                            int phase_phi, int parity, double dt, int ctr_off, cudaStream_t st);
+                            int phase_phi, int parity, double dt, int ctr_off, bool i32, cudaStream_t st);
 cudaError_t launch_batch_charge(const RepDesc *d, const EnsDyn *dyn, const int *rep, const int *first, int nblocks,
-                                int phase_q, int pass, double dt, int ctr_off_order, cudaStream_t st);
+                                int phase_q, int pass, double dt, int ctr_off_order, bool i32, cudaStream_t st);
 cudaError_t launch_batch_em(const RepDesc *d, const EnsDyn *dyn, const int *rep, const int *first, int nblocks,
                             int phase_phi, double dt, int ctr_off, cudaStream_t st);
 cudaError_t launch_ens_set(EnsDyn *dyn, unsigned long long ctr, double t, cudaStream_t st);

@@ -1373,26 +1373,40 @@ __device__ __forceinline__ void ideal_tile(const Fields &in, const Fields &out, 
     hyg = wrapn(y0 - 1 + hy, N);
   }
 
+  // Planes z0-1 .. z1 of the march, tracked incrementally (within two wraps
+  // of the buffer: nit <= Nz + 2), and rb_off split into its in-plane part
+  // and plane part, so the march does no integer division.
+  const int zfirst = z0 == 0 ? g.Nz - 1 : z0 - 1;
+  auto plane_of = [&](int q) {
+    int pl = zfirst + q;
+    if (pl >= g.Nz) pl -= g.Nz;
+    if (pl >= g.Nz) pl -= g.Nz;
+    return pl;
+  };
+  const long long NH = (long long)N * g.H;
+  const int own_xy = yj * g.H + (xi >> 1), own_par = (xi + yj) & 1;
+  const int ring_xy = hyg * g.H + (hxg >> 1), ring_par = (hxg + hyg) & 1;
   auto issue = [&](int plane, int stage, bool halo) {
-    const long long o = rb_off(g, xi, yj, plane);
+    const long long o = (long long)((own_par + plane) & 1) * g.V2 + (long long)plane * NH + own_xy;
 #pragma unroll
     for (int c = 0; c < 10; ++c) cp_async8(&raw[(stage * 10 + c) * SP + sc], in.c[c] + o);
     if (halo && hs >= 0) {
-      const long long oh = rb_off(g, hxg, hyg, plane);
+      const long long oh = (long long)((ring_par + plane) & 1) * g.V2 + (long long)plane * NH + ring_xy;
 #pragma unroll
       for (int c = 0; c < 10; ++c) cp_async8(&raw[(stage * 10 + c) * SP + hs], in.c[c] + oh);
     }
   };
 
-  issue(wrapn(z0 - 1, g.Nz), 0, false);
+  issue(zfirst, 0, false);
   cp_async_commit();
 
   double pm[4], pc[4], pn[4], qc[6], qn[6];
+  int pprev = zfirst;  // plane p - 1 (used from it >= 2)
   for (int it = 0; it < nit; ++it) {
-    const int p = wrapn(z0 - 1 + it, g.Nz);
+    const int p = plane_of(it);
     cp_async_wait_all();
     __syncthreads();
-    if (it + 1 < nit) issue(wrapn(p + 1, g.Nz), (it + 1) & 1, true);
+    if (it + 1 < nit) issue(plane_of(it + 1), (it + 1) & 1, true);
     cp_async_commit();
 
     const double *rw = raw + (it & 1) * 10 * SP;
@@ -1433,12 +1447,13 @@ __device__ __forceinline__ void ideal_tile(const Fields &in, const Fields &out, 
       // second half rotation on a copy: pc (phi') stays the z-1 neighbour of the next plane
       double pf[4] = {pc[0], pc[1], pc[2], pc[3]};
       rotate_site(pf, qc, a.dto2chi);
-      const long long o = rb_off(g, xi, yj, wrapn(p - 1, g.Nz));
+      const long long o = (long long)((own_par + pprev) & 1) * g.V2 + (long long)pprev * NH + own_xy;
 #pragma unroll
       for (int l = 0; l < 4; ++l) out.c[l][o] = pf[l];
 #pragma unroll
       for (int s = 0; s < 6; ++s) out.c[4 + s][o] = qc[s];
     }
+    pprev = p;
 #pragma unroll
     for (int l = 0; l < 4; ++l) {
       pm[l] = pc[l];
@@ -1815,6 +1830,7 @@ __device__ __forceinline__ bool slab_coords(const RepDesc &r, int local, int &m,
   return j < r.g.N;
 }
 
+template <typename I>
 __global__ void __launch_bounds__(128) batch_hb_kernel(const RepDesc *__restrict__ d, const EnsDyn *__restrict__ dyn,
                                                        const int *__restrict__ rep, const int *__restrict__ first,
                                                        int phase, int parity, double dt, int ctr_off) {
@@ -1834,10 +1850,11 @@ __global__ void __launch_bounds__(128) batch_hb_kernel(const RepDesc *__restrict
   // unrolled so the planes' loads and updates interleave (independent sites)
 #pragma unroll
   for (int q = 0; q < kBatchPlanes; ++q)
-    if (k0 + q < R.g.N) hb_site<false, false>(f, R.g, parity, a, m, j, k0 + q, mon);
+    if (k0 + q < R.g.N) hb_site<false, false, false, I>(f, R.g, parity, a, m, j, k0 + q, mon);
 }
 
 // 32 registers, full occupancy (as charge_pass_kernel)
+template <typename I>
 __global__ void __launch_bounds__(128, 16) batch_charge_kernel(const RepDesc *__restrict__ d,
                                                            const EnsDyn *__restrict__ dyn, const int *__restrict__ rep,
                                                            const int *__restrict__ first, int phase, int pass,
@@ -1868,7 +1885,7 @@ __global__ void __launch_bounds__(128, 16) batch_charge_kernel(const RepDesc *__
   MonLocal mon;
 #pragma unroll
   for (int q = 0; q < kBatchPlanes; ++q)
-    if (k0 + q < R.g.N) charge_link_site<false, false>(f, R.g, dir, eoA, a, m, j, k0 + q, mon);
+    if (k0 + q < R.g.N) charge_link_site<false, false, I>(f, R.g, dir, eoA, a, m, j, k0 + q, mon);
 }
 
 // ---- differentiable Euler-Maruyama runs of an ensemble ---------------------
@@ -2815,15 +2832,23 @@ cudaError_t launch_batch_ideal(const RepDesc *d, const int *rep, const int *firs
   return cudaGetLastError();
 }
 
+bool batch_idx32(const RepDesc *hd, int nrep) {
+  for (int r = 0; r < nrep; ++r)
+    if (!idx32(hd[r].g)) return false;
+  return true;
+}
+
 cudaError_t launch_batch_hb(const RepDesc *d, const EnsDyn *dyn, const int *rep, const int *first, int nblocks,
-                            int phase, int parity, double dt, int ctr_off, cudaStream_t st) {
-  batch_hb_kernel<<<nblocks, 128, 0, st>>>(d, dyn, rep, first, phase, parity, dt, ctr_off);
+                            int phase, int parity, double dt, int ctr_off, bool i32, cudaStream_t st) {
+  if (i32) batch_hb_kernel<int><<<nblocks, 128, 0, st>>>(d, dyn, rep, first, phase, parity, dt, ctr_off);
+  else batch_hb_kernel<long long><<<nblocks, 128, 0, st>>>(d, dyn, rep, first, phase, parity, dt, ctr_off);
   return cudaGetLastError();
 }
 
 cudaError_t launch_batch_charge(const RepDesc *d, const EnsDyn *dyn, const int *rep, const int *first, int nblocks,
-                                int phase, int pass, double dt, int ctr_off_order, cudaStream_t st) {
-  batch_charge_kernel<<<nblocks, 128, 0, st>>>(d, dyn, rep, first, phase, pass, dt, ctr_off_order);
+                                int phase, int pass, double dt, int ctr_off_order, bool i32, cudaStream_t st) {
+  if (i32) batch_charge_kernel<int><<<nblocks, 128, 0, st>>>(d, dyn, rep, first, phase, pass, dt, ctr_off_order);
+  else batch_charge_kernel<long long><<<nblocks, 128, 0, st>>>(d, dyn, rep, first, phase, pass, dt, ctr_off_order);
   return cudaGetLastError();
 }
 
