@@ -65,6 +65,7 @@ def parse():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--no-postprocess", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the 64^3 Model G run and the z-slab emulation")
     return ap.parse_args()
 
 
@@ -879,7 +880,7 @@ def run_ours(a):
         adjoint["batched"] = run_adjoint_batch()
     model_g_64 = None
     slab = None
-    if world == 1 and not a.no_variants:
+    if world == 1 and not a.no_variants and not a.no_extras:
         model_g_64 = run_model_g_64()
         slab = run_slab_emulated()
     postprocess = None
