@@ -241,7 +241,8 @@ ENS_H = (0.003, 0.006, 0.012)
 def run_ensemble(steps=20, plain_steps=2):
     """Batched ensemble (one launch per sub-step over all replicas, autotuned,
     two-step CUDA graphs) vs looping the single-lattice path one replica per
-    launch.  Returns replica-steps/s of both."""
+    launch, and the same ensemble as one persistent launch per step.  Returns
+    replica-steps/s of the batched and plain forms and the persistent step time."""
     import ctypes as C
 
     import torch
@@ -274,6 +275,17 @@ def run_ensemble(steps=20, plain_steps=2):
     e1.record(stream)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / steps
+    # the same steps as one persistent (cooperative) launch per step
+    persistent_ms = None
+    if lib.lgv_ensemble_use_persistent(e, 1) == L.LGV_OK:
+        L.check(lib.lgv_ensemble_step(e, L.PV2HBSPLIT, 2, 3, DT, 0.0, 4), "warm persistent")
+        torch.cuda.synchronize()
+        e0.record(stream)
+        L.check(lib.lgv_ensemble_step(e, L.PV2HBSPLIT, 2, 3, DT, 0.0, steps), "persistent step")
+        e1.record(stream)
+        torch.cuda.synchronize()
+        L.check(lib.lgv_ensemble_synchronize(e), "persistent sync")
+        persistent_ms = e0.elapsed_time(e1) / steps
     lib.lgv_ensemble_destroy(e)
 
     plain = {}
@@ -314,7 +326,10 @@ def run_ensemble(steps=20, plain_steps=2):
                             "packing": ["given", "largest_first", "interleaved"][choice[2]]},
         "plain_ms_per_step": plain, "plain_replica_steps_per_s": R / (best_plain / 1e3),
         "speedup_vs_plain": best_plain / ms,
-        "timing": "batched: CUDA events over graph replays; plain: host wall clock around a loop of lgv_step, "
+        "persistent_ms_per_step": persistent_ms,
+        "persistent_over_batched": (persistent_ms / ms) if persistent_ms else None,
+        "timing": "batched: CUDA events over graph replays; persistent: the same with one cooperative launch per "
+                  "step (lgv_ensemble_use_persistent); plain: host wall clock around a loop of lgv_step, "
                   "one replica per call (one shared stream / each handle on its own stream), best of three rounds",
     }
 
@@ -374,7 +389,8 @@ def run_slab_emulated(N=256, R=2, steps=5):
     h = C.c_void_p()
     L.check(lib.lgv_create(C.byref(p), C.byref(h)), "create")
     try:
-        L.check(lib.lgv_set_state(h, L.ptr(np.ascontiguousarray(u))), "set_state")
+        u = np.ascontiguousarray(u)  # held while the call reads it
+        L.check(lib.lgv_set_state(h, L.ptr(u)), "set_state")
         L.check(lib.lgv_step(h, L.PV2HBSPLIT, 2, 3, DT, 0.0, 1), "warm")
         L.check(lib.lgv_synchronize(h), "sync")
         t0 = time.perf_counter()

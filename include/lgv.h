@@ -290,6 +290,16 @@ int lgv_ensemble_autotune(lgv_ensemble *e, int evolver, int inner, int outer, do
  * ensemble's own stream and replayed on its current stream, which may be any
  * stream the caller set, the legacy default stream included. */
 int lgv_ensemble_use_graphs(lgv_ensemble *e, int enable);
+/* One persistent launch per step (off by default; LGV_ENS_PERSISTENT=1 in the
+ * environment at lgv_ensemble_create turns it on): a cooperative launch of
+ * two 256-thread CTAs per SM runs every sub-step of the step over all
+ * replicas, the sub-steps separated by a grid barrier whose waits are bounded
+ * (a wait that gives up is reported as LGV_ERR_TIMEOUT by the next
+ * synchronising call), and is captured in the CUDA graphs as any other launch.
+ * Same results as the default one launch per sub-step, bit for bit.  The
+ * Euler-Maruyama evolver keeps its own launch.  LGV_ERR_UNSUPPORTED when the
+ * device has no cooperative launch. */
+int lgv_ensemble_use_persistent(lgv_ensemble *e, int enable);
 /* Differentiable Euler-Maruyama Model A runs of all replicas at once (no
  * counterpart in the reference): one launch per step over all replicas.
  * Replica r gets what lgv_diff_forward / lgv_diff_backward with evolver

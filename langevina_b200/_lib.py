@@ -106,6 +106,7 @@ SIGNATURES = [
     ("lgv_ensemble_use_graphs", C.c_int, [_H, C.c_int]),
     ("lgv_ensemble_diff_forward", C.c_int, [_H, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, C.c_void_p]),
     ("lgv_ensemble_diff_backward", C.c_int, [_H, C.c_void_p, C.c_void_p]),
+    ("lgv_ensemble_use_persistent", C.c_int, [_H, C.c_int]),
     ("lgv_ensemble_set_stream", C.c_int, [_H, C.c_void_p]),
     ("lgv_ensemble_synchronize", C.c_int, [_H]),
     ("lgv_slab_create", C.c_int, [C.POINTER(lgv_params), C.c_int, C.c_int, C.POINTER(_H)]),

@@ -88,6 +88,11 @@ struct lgv_ensemble {
   cudaStream_t side = nullptr;
   // every replica's element offsets fit 31 bits (set at creation)
   bool idx32 = false;
+  // one cooperative launch per step instead of one launch per sub-step
+  // (lgv_ensemble_use_persistent; LGV_ENS_PERSISTENT=1 at creation), and its
+  // grid barrier (arrivals, generation, error flag)
+  bool persistent = false;
+  unsigned *bar = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;
   // differentiable Euler-Maruyama run (lgv_ensemble_diff_forward / _backward)
   struct {
@@ -119,6 +124,7 @@ int ens_check_waits(lgv_ensemble *e) {
   ECK(cudaStreamSynchronize(e->stream));
   if (n) {
     ECK(cudaMemsetAsync(e->waits, 0, sizeof(n), e->stream));
+    if (e->bar) ECK(cudaMemsetAsync(e->bar, 0, 3 * sizeof(unsigned), e->stream));  // a barrier that gave up
     return efail(LGV_ERR_TIMEOUT, "bounded device waits timed out: " + std::to_string(n) +
                                       " TMA copy waits of the ideal step; the ensemble state is not valid");
   }
@@ -256,8 +262,94 @@ int step_ctr(int ev, int inner, int outer) {
   }
 }
 
+// Sub-step phases of one step (the persistent launch's plan), or -1 for an
+// evolver it does not run (Euler-Maruyama keeps its own kernel).
+int persist_phases(int ev, int inner, int outer) {
+  switch (ev) {
+    case LGV_PV2HBSPLIT: return outer * (1 + 2 * inner) + 6;
+    case LGV_PV2HBSPLIT_NODIFFUSE: return outer * (1 + 2 * inner);
+    case LGV_PV2HBSPLIT_ONLYDIFFUSE: return 6;
+    case LGV_IDEAL_PV2: return 1;
+    case LGV_EULER_LANGEVIN_HB: return 2;
+    case LGV_CHARGE_HB: return 6;
+    default: return -1;
+  }
+}
+
+// One step as one cooperative launch (lgv::launch_ens_persistent): the same
+// sub-steps, buffer phases and counter offsets as enqueue_step below, as the
+// phases of a plan.
+int enqueue_step_persistent(lgv_ensemble *e, int ev, int inner, int outer, double dt) {
+  lgv::PersistPlan P{};
+  P.nb_tma = e->tma_map.nblocks;
+  P.nb_cp = e->ideal_map.nblocks;
+  P.nb_slab = e->slab_map.nblocks;
+  P.tile = e->tile;
+  P.wait_limit = e->wait_limit;
+  int off = 0;
+  auto add = [&](int kind, int arg, double d) {
+    lgv::PersistPhase &ph = P.ph[P.nphase++];
+    ph.kind = kind;
+    ph.arg = arg;
+    ph.pphi = e->phase_phi;
+    ph.pq = e->phase_q;
+    ph.ctr_off = off;
+    ph.dt = d;
+  };
+  auto ideal = [&](double d) {
+    add(lgv::kPersistIdeal, 0, d);
+    e->phase_phi ^= 1;
+    e->phase_q ^= 1;
+  };
+  auto hb = [&](double d) {
+    for (int parity = 0; parity < 2; ++parity) add(lgv::kPersistPhi, parity, d);
+    off += 1;
+  };
+  auto charge = [&](double d) {
+    for (int pass = 0; pass < 6; ++pass) add(lgv::kPersistCharge, pass, d);
+    off += 7;
+  };
+  switch (ev) {
+    case LGV_PV2HBSPLIT:
+    case LGV_PV2HBSPLIT_NODIFFUSE:
+    case LGV_PV2HBSPLIT_ONLYDIFFUSE:
+      if (ev != LGV_PV2HBSPLIT_ONLYDIFFUSE)
+        for (int i1 = 0; i1 < outer; ++i1) {
+          ideal(dt / (unsigned)outer);
+          for (int i0 = 0; i0 < inner; ++i0) hb(dt / ((unsigned)inner * (unsigned)outer));
+        }
+      if (ev != LGV_PV2HBSPLIT_NODIFFUSE) charge(dt);
+      break;
+    case LGV_IDEAL_PV2: ideal(dt); break;
+    case LGV_EULER_LANGEVIN_HB: hb(dt); break;
+    case LGV_CHARGE_HB: charge(dt); break;
+    default: return efail(LGV_ERR_INVALID, "ensemble: evolver without a persistent plan");
+  }
+  P.dctr = (unsigned long long)off;
+  P.dt_step = dt;
+  lgv::PersistPtrs q{};
+  q.d = e->dd;
+  q.dyn = e->dyn;
+  q.gmaps = e->gmaps;
+  q.tma_rep = e->tma_map.rep;
+  q.tma_first = e->tma_map.first;
+  q.cp_rep = e->ideal_map.rep;
+  q.cp_first = e->ideal_map.first;
+  q.slab_rep = e->slab_map.rep;
+  q.slab_first = e->slab_map.first;
+  q.waits = e->waits;
+  q.bar = e->bar;
+  ECK(lgv::launch_ens_persistent(P, q, e->idx32, e->stream));
+  e->ctr += (unsigned long long)off;
+  return LGV_OK;
+}
+
 // Enqueue one step on e->stream (also used inside graph capture).
 int enqueue_step(lgv_ensemble *e, int ev, int inner, int outer, double dt) {
+  if (e->persistent) {
+    const int np = persist_phases(ev, inner, outer);
+    if (np > 0 && np <= lgv::kMaxPersistPhases) return enqueue_step_persistent(e, ev, inner, outer, dt);
+  }
   const int nb_i = e->ideal_map.nblocks, nb_p = e->plane_map.nblocks, nb_s = e->slab_map.nblocks;
   int off = 0;
   auto ideal = [&](double d) -> int {
@@ -400,6 +492,13 @@ int lgv_ensemble_create(int nrep, const lgv_params *params, lgv_ensemble **out) 
     }
   }
   e->idx32 = lgv::batch_idx32(e->hd.data(), nrep);
+  if (cudaMalloc((void **)&e->bar, 3 * sizeof(unsigned)) != cudaSuccess ||
+      cudaMemset(e->bar, 0, 3 * sizeof(unsigned)) != cudaSuccess)
+    return bail(efail(LGV_ERR_NOMEM, "grid barrier"));
+  {
+    const char *pv = std::getenv("LGV_ENS_PERSISTENT");
+    e->persistent = pv && pv[0] == '1' && lgv::persist_grid(e->idx32) > 0;
+  }
   if (cudaMalloc((void **)&e->dd, nrep * sizeof(RepDesc)) != cudaSuccess ||
       cudaMalloc((void **)&e->dyn, sizeof(EnsDyn)) != cudaSuccess ||
       cudaMalloc((void **)&e->oavg, (size_t)nrep * 11 * sizeof(double)) != cudaSuccess)
@@ -433,6 +532,7 @@ int lgv_ensemble_destroy(lgv_ensemble *e) {
   if (e->diff.partial) cudaFree(e->diff.partial);
   if (e->diff.done) cudaFree(e->diff.done);
   if (e->waits) cudaFree(e->waits);
+  if (e->bar) cudaFree(e->bar);
   if (e->side) {
     cudaStreamSynchronize(e->side);
     cudaStreamDestroy(e->side);
@@ -724,6 +824,18 @@ int lgv_ensemble_tune(lgv_ensemble *e, int tile, int zchunk, int order) {
 int lgv_ensemble_use_graphs(lgv_ensemble *e, int enable) {
   if (!e) return efail(LGV_ERR_INVALID, "ensemble is NULL");
   e->graphs = enable != 0;
+  return LGV_OK;
+}
+
+int lgv_ensemble_use_persistent(lgv_ensemble *e, int enable) {
+  if (!e) return efail(LGV_ERR_INVALID, "ensemble is NULL");
+  if (enable && lgv::persist_grid(e->idx32) <= 0)
+    return efail(LGV_ERR_UNSUPPORTED, "persistent ensemble step: no cooperative launch on this device");
+  if ((enable != 0) != e->persistent) {
+    ECK(cudaStreamSynchronize(e->stream));
+    clear_graphs(e);
+  }
+  e->persistent = enable != 0;
   return LGV_OK;
 }
 

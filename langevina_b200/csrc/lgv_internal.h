@@ -148,6 +148,41 @@ cudaError_t launch_batch_oavg_final(const RepDesc *d, const int *first, const in
                                     const double *partial, double *out, cudaStream_t st);
 int ideal_tile_dims(int tile, int *tx, int *ty);
 
+// ---- persistent ensemble step ----------------------------------------------
+// One cooperative launch runs every sub-step of a step over all replicas, as
+// phases separated by a grid barrier: the ideal step (TMA replicas' tiles,
+// then cp.async replicas' tiles), a phi parity pass or a charge face, each
+// over the same block maps as the one-launch-per-sub-step path.
+enum PersistKind { kPersistIdeal = 0, kPersistPhi = 1, kPersistCharge = 2 };
+struct PersistPhase {
+  int kind;       // PersistKind
+  int arg;        // parity (phi pass) or pass 0..5 (charge face)
+  int pphi, pq;   // buffers holding the current phi / charges
+  int ctr_off;    // counter offset of the sub-step within the step
+  double dt;      // the sub-step's dt
+};
+constexpr int kMaxPersistPhases = 64;
+struct PersistPlan {
+  int nphase;
+  int nb_tma, nb_cp, nb_slab;  // blocks of the TMA ideal, cp.async ideal and slab maps
+  int tile;                    // cp.async ideal tile (LGV_TILE_*)
+  int wait_limit;              // polls before a device wait gives up
+  unsigned long long dctr;     // counter advance of the step
+  double dt_step;              // clock advance of the step
+  PersistPhase ph[kMaxPersistPhases];
+};
+struct PersistPtrs {
+  const RepDesc *d;
+  EnsDyn *dyn;
+  const void *gmaps;
+  const int *tma_rep, *tma_first, *cp_rep, *cp_first, *slab_rep, *slab_first;
+  unsigned long long *waits;  // bounded waits that gave up (barrier or TMA)
+  unsigned *bar;              // grid barrier: arrivals, generation, error (zeroed)
+};
+// CTAs of the launch (resident at once): 0 when a cooperative launch is not possible
+int persist_grid(bool i32);
+cudaError_t launch_ens_persistent(const PersistPlan &plan, const PersistPtrs &q, bool i32, cudaStream_t st);
+
 // ---------------------------------------------------------------------------
 // Adjoint of the Euler-Maruyama Model A step (noise held fixed).
 struct EmAdjArgs {

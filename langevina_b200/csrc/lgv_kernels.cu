@@ -23,6 +23,7 @@
 //   em_adjoint_kernel, rot_phi_kernel, ideal_adj_a/b_kernel, batch_em_*
 //                       adjoints of the Euler-Maruyama and ideal steps for the
 //                       differentiable runs (no counterpart)
+#include "lgv_ideal_tma_cta.cuh"
 #include "lgv_internal.h"
 
 #include <algorithm>
@@ -1821,24 +1822,27 @@ __device__ __forceinline__ bool plane_coords(const RepDesc &r, int local, int &m
 // consecutive planes of one replica, so the block-map and descriptor loads
 // (two dependent round trips before the first site load) are paid once per
 // kBatchPlanes planes
-__device__ __forceinline__ bool slab_coords(const RepDesc &r, int local, int &m, int &j, int &k0) {
+__device__ __forceinline__ bool slab_coords(const RepDesc &r, int local, int lane, int &m, int &j, int &k0) {
   const int chunk = local % r.nchunk;
   k0 = (local / r.nchunk) * kBatchPlanes;
-  const int t = chunk * 128 + (int)threadIdx.x;
+  const int t = chunk * 128 + lane;
   j = t / r.g.H;
   m = t - j * r.g.H;
   return j < r.g.N;
 }
 
+// Items of the batched heat-bath and charge sub-steps: block blk of the slab
+// map, lane 0..127 of its 128 threads (a kernel of their own, or half of a
+// CTA of the persistent step).
 template <typename I>
-__global__ void __launch_bounds__(128) batch_hb_kernel(const RepDesc *__restrict__ d, const EnsDyn *__restrict__ dyn,
-                                                       const int *__restrict__ rep, const int *__restrict__ first,
-                                                       int phase, int parity, double dt, int ctr_off) {
-  const int r = rep[blockIdx.x];
+__device__ __forceinline__ void batch_hb_item(const RepDesc *__restrict__ d, const EnsDyn *__restrict__ dyn,
+                                              const int *__restrict__ rep, const int *__restrict__ first, int blk,
+                                              int lane, int phase, int parity, double dt, int ctr_off) {
+  const int r = rep[blk];
   const RepDesc &R = d[r];
   const EnsDyn y = *dyn;
   int m, j, k0;
-  if (!slab_coords(R, blockIdx.x - first[r], m, j, k0)) return;
+  if (!slab_coords(R, blk - first[r], lane, m, j, k0)) return;
   HbArgs a{};
   a.rdtg = sqrt(2. * dt * R.gamma);
   a.Lambda2 = 0.5 * (2. * 3. + rep_mass(R, y));
@@ -1853,17 +1857,22 @@ __global__ void __launch_bounds__(128) batch_hb_kernel(const RepDesc *__restrict
     if (k0 + q < R.g.N) hb_site<false, false, false, I>(f, R.g, parity, a, m, j, k0 + q, mon);
 }
 
-// 32 registers, full occupancy (as charge_pass_kernel)
 template <typename I>
-__global__ void __launch_bounds__(128, 16) batch_charge_kernel(const RepDesc *__restrict__ d,
-                                                           const EnsDyn *__restrict__ dyn, const int *__restrict__ rep,
-                                                           const int *__restrict__ first, int phase, int pass,
-                                                           double dt, int ctr_off_order) {
-  const int r = rep[blockIdx.x];
+__global__ void __launch_bounds__(128) batch_hb_kernel(const RepDesc *__restrict__ d, const EnsDyn *__restrict__ dyn,
+                                                       const int *__restrict__ rep, const int *__restrict__ first,
+                                                       int phase, int parity, double dt, int ctr_off) {
+  batch_hb_item<I>(d, dyn, rep, first, blockIdx.x, threadIdx.x, phase, parity, dt, ctr_off);
+}
+
+template <typename I>
+__device__ __forceinline__ void batch_charge_item(const RepDesc *__restrict__ d, const EnsDyn *__restrict__ dyn,
+                                                  const int *__restrict__ rep, const int *__restrict__ first, int blk,
+                                                  int lane, int phase, int pass, double dt, int ctr_off_order) {
+  const int r = rep[blk];
   const RepDesc &R = d[r];
   const EnsDyn y = *dyn;
   int m, j, k0;
-  if (!slab_coords(R, blockIdx.x - first[r], m, j, k0)) return;
+  if (!slab_coords(R, blk - first[r], lane, m, j, k0)) return;
   // the replica's pass order (counter mode of ModelGChargeHB::step)
   const unsigned long long c0 = y.ctr + (unsigned long long)ctr_off_order;
   const uint64_t w = split_word(sub_key(R.key, c0), 0);
@@ -1886,6 +1895,15 @@ __global__ void __launch_bounds__(128, 16) batch_charge_kernel(const RepDesc *__
 #pragma unroll
   for (int q = 0; q < kBatchPlanes; ++q)
     if (k0 + q < R.g.N) charge_link_site<false, false, I>(f, R.g, dir, eoA, a, m, j, k0 + q, mon);
+}
+
+// 32 registers, full occupancy (as charge_pass_kernel)
+template <typename I>
+__global__ void __launch_bounds__(128, 16) batch_charge_kernel(const RepDesc *__restrict__ d,
+                                                           const EnsDyn *__restrict__ dyn, const int *__restrict__ rep,
+                                                           const int *__restrict__ first, int phase, int pass,
+                                                           double dt, int ctr_off_order) {
+  batch_charge_item<I>(d, dyn, rep, first, blockIdx.x, threadIdx.x, phase, pass, dt, ctr_off_order);
 }
 
 // ---- differentiable Euler-Maruyama runs of an ensemble ---------------------
@@ -2054,13 +2072,11 @@ __global__ void __launch_bounds__(128) batch_em_kernel(const RepDesc *__restrict
 }
 
 template <int TX, int TY>
-__global__ void __launch_bounds__(TX *TY, 2) batch_ideal_kernel(const RepDesc *__restrict__ d,
-                                                                const int *__restrict__ rep,
-                                                                const int *__restrict__ first, int pphi, int pq,
-                                                                double dt) {
-  const int r = rep[blockIdx.x];
+__device__ __forceinline__ void batch_ideal_item(const RepDesc *__restrict__ d, const int *__restrict__ rep,
+                                                 const int *__restrict__ first, int blk, int pphi, int pq, double dt) {
+  const int r = rep[blk];
   const RepDesc &R = d[r];
-  const int l = blockIdx.x - first[r];
+  const int l = blk - first[r];
   const int bx = l % R.igx, by = (l / R.igx) % R.igy, bz = l / (R.igx * R.igy);
   IdealArgs a;
   a.dto2chi = (dt / 2.0) / R.chi;
@@ -2068,6 +2084,137 @@ __global__ void __launch_bounds__(TX *TY, 2) batch_ideal_kernel(const RepDesc *_
   a.a2 = R.a2;
   a.H = R.H;
   ideal_tile<TX, TY>(rep_fields(R, pphi, pq), rep_fields(R, pphi ^ 1, pq ^ 1), R.g, R.izc, a, bx, by, bz);
+}
+
+template <int TX, int TY>
+__global__ void __launch_bounds__(TX *TY, 2) batch_ideal_kernel(const RepDesc *__restrict__ d,
+                                                                const int *__restrict__ rep,
+                                                                const int *__restrict__ first, int pphi, int pq,
+                                                                double dt) {
+  batch_ideal_item<TX, TY>(d, rep, first, blockIdx.x, pphi, pq, dt);
+}
+
+// ---- persistent ensemble step -------------------------------------------------
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Grid barrier over the co-resident CTAs of a cooperative launch.  bar[0]
+// counts the arrivals of the current generation, bar[1] is the generation and
+// bar[2] an error flag.  One thread per CTA reads the generation, publishes
+// the CTA's writes (fence) and arrives; the last to arrive resets the count
+// and advances the generation, the others poll it -- at most `limit` times,
+// after which the CTA raises the error flag, counts a timed-out wait and
+// gives up.  A CTA that sees the error flag gives up too, so every CTA leaves
+// the launch after a bounded number of polls whatever happened to the
+// others.  Returns false when the launch should stop.
+__device__ __forceinline__ bool grid_barrier(unsigned *bar, unsigned nblocks, int limit, unsigned long long *waits) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    const unsigned gen = ld_acquire_u32(bar + 1);
+    __threadfence();
+    if (atomicAdd(bar, 1u) == nblocks - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      for (int i = 0;; ++i) {
+        if (ld_acquire_u32(bar + 1) != gen) break;
+        if (ld_acquire_u32(bar + 2) != 0u) {
+          ok = 0;
+          break;
+        }
+        if (i >= limit) {
+          ok = 0;
+          atomicExch(bar + 2, 1u);
+          if (waits) atomicAdd(waits, 1ull);
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+constexpr size_t kPersistSmem = (tma::kSmemBytes > IdealTile<32, 8>::SMEM)
+                                    ? (tma::kSmemBytes > IdealTile<16, 16>::SMEM ? tma::kSmemBytes
+                                                                                 : IdealTile<16, 16>::SMEM)
+                                    : (IdealTile<32, 8>::SMEM > IdealTile<16, 16>::SMEM ? IdealTile<32, 8>::SMEM
+                                                                                        : IdealTile<16, 16>::SMEM);
+
+// The persistent step's bodies as calls, so that each keeps the register
+// allocation of its own kernel instead of the union of all of them.
+__device__ __noinline__ void persist_tma_tile(const PersistPtrs &q, int w, const PersistPhase &ph, int limit) {
+  tma::batch_tma_item(q.d, reinterpret_cast<const CUtensorMap *>(q.gmaps), q.tma_rep, q.tma_first, w, ph.pphi, ph.pq,
+                      ph.dt, q.waits, limit);
+}
+template <int TX, int TY>
+__device__ __noinline__ void persist_cp_tile(const PersistPtrs &q, int w, const PersistPhase &ph) {
+  batch_ideal_item<TX, TY>(q.d, q.cp_rep, q.cp_first, w, ph.pphi, ph.pq, ph.dt);
+}
+template <typename I>
+__device__ __noinline__ void persist_phi_item(const PersistPtrs &q, int blk, int lane, const PersistPhase &ph) {
+  batch_hb_item<I>(q.d, q.dyn, q.slab_rep, q.slab_first, blk, lane, ph.pphi, ph.arg, ph.dt, ph.ctr_off);
+}
+template <typename I>
+__device__ __noinline__ void persist_charge_item(const PersistPtrs &q, int blk, int lane, const PersistPhase &ph) {
+  batch_charge_item<I>(q.d, q.dyn, q.slab_rep, q.slab_first, blk, lane, ph.pq, ph.arg, ph.dt, ph.ctr_off);
+}
+
+// One step of an ensemble in one launch of 256-thread CTAs, two per SM (the
+// ideal step's CTA bodies set the shape).  Each phase hands its items out
+// round robin over the grid: ideal tiles (TMA replicas first, through the
+// same CTA bodies as batch_ideal_tma_kernel and batch_ideal_kernel), or pairs
+// of 128-lane slab items of the heat-bath and charge sub-steps (each half of
+// the CTA one item, as batch_hb_kernel / batch_charge_kernel).  Phases are
+// separated by grid_barrier; after the last one block 0 advances the
+// ensemble's counter and clock, as launch_ens_advance does after the
+// one-launch-per-sub-step sequence.  Results equal that sequence's bit for
+// bit (same device functions, same noise indexing).
+template <typename I>
+__global__ void __launch_bounds__(256, 2) ens_persistent_kernel(const __grid_constant__ PersistPlan P,
+                                                                const PersistPtrs q) {
+  const int lane = threadIdx.x & 127, half = threadIdx.x >> 7;
+  for (int f = 0; f < P.nphase; ++f) {
+    const PersistPhase &ph = P.ph[f];
+    if (ph.kind == kPersistIdeal) {
+      const int n = P.nb_tma + P.nb_cp;
+      for (int w = blockIdx.x; w < n; w += gridDim.x) {
+        if (w < P.nb_tma) {
+          // the TMA loads (async proxy) read what the previous phase stored
+          if (threadIdx.x == 0) asm volatile("fence.proxy.async.global;\n" ::: "memory");
+          persist_tma_tile(q, w, ph, P.wait_limit);
+        } else if (P.tile == LGV_TILE_16x16) {
+          persist_cp_tile<16, 16>(q, w - P.nb_tma, ph);
+        } else {
+          persist_cp_tile<32, 8>(q, w - P.nb_tma, ph);
+        }
+        __syncthreads();  // the tile's shared memory and barriers are reused by the next one
+      }
+    } else {
+      const int n = (P.nb_slab + 1) / 2;
+      for (int w = blockIdx.x; w < n; w += gridDim.x) {
+        const int blk = 2 * w + half;
+        if (blk < P.nb_slab) {
+          if (ph.kind == kPersistPhi) persist_phi_item<I>(q, blk, lane, ph);
+          else persist_charge_item<I>(q, blk, lane, ph);
+        }
+      }
+    }
+    if (!grid_barrier(q.bar, gridDim.x, P.wait_limit, q.waits)) return;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    q.dyn->ctr += P.dctr;
+    q.dyn->t += P.dt_step;
+  }
 }
 
 __global__ void ens_set_kernel(EnsDyn *dyn, unsigned long long ctr, double t) {
@@ -2850,6 +2997,31 @@ cudaError_t launch_batch_charge(const RepDesc *d, const EnsDyn *dyn, const int *
   if (i32) batch_charge_kernel<int><<<nblocks, 128, 0, st>>>(d, dyn, rep, first, phase, pass, dt, ctr_off_order);
   else batch_charge_kernel<long long><<<nblocks, 128, 0, st>>>(d, dyn, rep, first, phase, pass, dt, ctr_off_order);
   return cudaGetLastError();
+}
+
+int persist_grid(bool i32) {
+  static int cached[2] = {-1, -1};
+  int &c = cached[i32 ? 1 : 0];
+  if (c >= 0) return c;
+  c = 0;
+  int dev = 0, coop = 0, sms = 0, per = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop) return 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+  const void *kern = i32 ? (const void *)ens_persistent_kernel<int> : (const void *)ens_persistent_kernel<long long>;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPersistSmem) != cudaSuccess)
+    return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 256, kPersistSmem) != cudaSuccess) return 0;
+  c = per * sms;
+  return c;
+}
+
+cudaError_t launch_ens_persistent(const PersistPlan &plan, const PersistPtrs &q, bool i32, cudaStream_t st) {
+  const int grid = persist_grid(i32);
+  if (grid <= 0) return cudaErrorCooperativeLaunchTooLarge;
+  const void *kern = i32 ? (const void *)ens_persistent_kernel<int> : (const void *)ens_persistent_kernel<long long>;
+  void *args[] = {const_cast<PersistPlan *>(&plan), const_cast<PersistPtrs *>(&q)};
+  return cudaLaunchCooperativeKernel(kern, grid, 256, args, kPersistSmem, st);
 }
 
 cudaError_t launch_batch_em(const RepDesc *d, const EnsDyn *dyn, const int *rep, const int *first, int nblocks,

@@ -127,7 +127,8 @@ class GpuLattice:
                      "inject_charge")
 
     def inject_em(self, xi):
-        self.L.check(self.lib.lgv_inject_em(self.h, self.L.ptr(np.ascontiguousarray(xi))), "inject_em")
+        xi = np.ascontiguousarray(xi)  # held while the call reads it
+        self.L.check(self.lib.lgv_inject_em(self.h, self.L.ptr(xi)), "inject_em")
 
     def step(self, ev, dt, t=0.0, nsteps=1, inner=1, outer=1):
         self.L.check(self.lib.lgv_step(self.h, ev, inner, outer, float(dt), float(t), int(nsteps)), "step")
