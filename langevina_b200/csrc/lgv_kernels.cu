@@ -1206,16 +1206,17 @@ __global__ void __launch_bounds__(kSlabThreads) charge_slab_kernel(Fields in, Fi
 
 // ----------------------------------------------------------------------------
 // Euler-Maruyama Model A step (Jacobi: reads `in`, writes phi of `out`).
-// One thread per element m of both parity half-rows of row (j, k).
-template <bool INJECTED>
+// One thread per element m of both parity half-rows of row (j, k).  I: the
+// element offset type (int when idx32 holds, as the heat-bath pass).
+template <bool INJECTED, typename I = long long>
 __device__ __forceinline__ void em_pair(const Fields &in, const Fields &out, const Geo &g, const EmArgs &a, int m,
                                         int j, int k, double (&acc)[4]) {
   const int H = g.H, N = g.N;
-  const long long row = ((long long)k * N + j) * H;
-  const long long rjp = ((long long)k * N + wrap_inc(j, N)) * H;
-  const long long rjm = ((long long)k * N + wrap_dec(j, N)) * H;
-  const long long rkp = ((long long)wrap_inc(k, g.Nz) * N + j) * H;
-  const long long rkm = ((long long)wrap_dec(k, g.Nz) * N + j) * H;
+  const I row = ((I)k * N + j) * H;
+  const I rjp = ((I)k * N + wrap_inc(j, N)) * H + m;
+  const I rjm = ((I)k * N + wrap_dec(j, N)) * H + m;
+  const I rkp = ((I)wrap_inc(k, g.Nz) * N + j) * H + m;
+  const I rkm = ((I)wrap_dec(k, g.Nz) * N + j) * H + m;
 #pragma unroll
   for (int parity = 0; parity < 2; ++parity) {
     const int s = (parity + j + k) & 1;
@@ -1223,9 +1224,10 @@ __device__ __forceinline__ void em_pair(const Fields &in, const Fields &out, con
     int xm = m - 1 + s, xp = m + s;
     if (xm < 0) xm += H;
     if (xp == H) xp = 0;
-    const long long own = (long long)parity * g.V2 + row + m;
-    const long long ob = (long long)(parity ^ 1) * g.V2;
-    const long long nat = nat_index(g, i, j, k);
+    const I own = (I)parity * (I)g.V2 + row + m;
+    const I ob = (I)(parity ^ 1) * (I)g.V2;
+    const I orow = ob + row;
+    const long long nat = (long long)nat_index_t<I>(g, i, j, k);
     double xi[4];
     if (INJECTED) {
 #pragma unroll
@@ -1243,8 +1245,7 @@ __device__ __forceinline__ void em_pair(const Fields &in, const Fields &out, con
 #pragma unroll
     for (int l = 0; l < 4; ++l) {
       const double *P = in.c[l];
-      const double heff = (P[ob + row + xp] + P[ob + row + xm]) + (P[ob + rjp + m] + P[ob + rjm + m]) +
-                          (P[ob + rkp + m] + P[ob + rkm + m]);
+      const double heff = (P[orow + xp] + P[orow + xm]) + (P[ob + rjp] + P[ob + rjm]) + (P[ob + rkp] + P[ob + rkm]);
       double fo = -heff + a.c6 * c[l] + a.lambda * p2 * c[l];
       if (l == 0) fo -= a.H;
       const double v = c[l] - a.dtg * fo + a.sq * xi[l];
@@ -1257,7 +1258,7 @@ __device__ __forceinline__ void em_pair(const Fields &in, const Fields &out, con
 // One thread per site pair (element m of both parity half rows of row (j, k)),
 // flat over the V/2 pairs.  AVG: also the volume averages of the new phi into
 // avg_out[0..3] (grid_sum4).
-template <bool INJECTED, bool AVG>
+template <bool INJECTED, bool AVG, typename I>
 __global__ void __launch_bounds__(kThreads, 4) em_kernel(Fields in, Fields out, Geo g, EmArgs a, double *partial,
                                                       unsigned *done, double *avg_out) {
   const long long idx = (long long)blockIdx.x * kThreads + threadIdx.x;
@@ -1265,7 +1266,7 @@ __global__ void __launch_bounds__(kThreads, 4) em_kernel(Fields in, Fields out, 
   if (idx < g.V2) {
     int m, j, k;
     pair_coords(idx, g, m, j, k);
-    em_pair<INJECTED>(in, out, g, a, m, j, k, acc);
+    em_pair<INJECTED, I>(in, out, g, a, m, j, k, acc);
   }
   if (AVG) grid_sum4<kThreads>(acc, partial, done, avg_out, 1.0 / (2.0 * (double)g.V2), false);
 }
@@ -2851,8 +2852,14 @@ cudaError_t launch_em(Fields in, Fields out, int N, const EmArgs &a, cudaStream_
 
 cudaError_t launch_em(Fields in, Fields out, const Geo &g, const EmArgs &a, cudaStream_t st) {
   const unsigned nb = nblocks(g.V2, kThreads);
-  if (a.xi) em_kernel<true, false><<<nb, kThreads, 0, st>>>(in, out, g, a, nullptr, nullptr, nullptr);
-  else em_kernel<false, false><<<nb, kThreads, 0, st>>>(in, out, g, a, nullptr, nullptr, nullptr);
+  const bool i32 = idx32(g);
+  if (a.xi) {
+    if (i32) em_kernel<true, false, int><<<nb, kThreads, 0, st>>>(in, out, g, a, nullptr, nullptr, nullptr);
+    else em_kernel<true, false, long long><<<nb, kThreads, 0, st>>>(in, out, g, a, nullptr, nullptr, nullptr);
+  } else {
+    if (i32) em_kernel<false, false, int><<<nb, kThreads, 0, st>>>(in, out, g, a, nullptr, nullptr, nullptr);
+    else em_kernel<false, false, long long><<<nb, kThreads, 0, st>>>(in, out, g, a, nullptr, nullptr, nullptr);
+  }
   return cudaGetLastError();
 }
 
@@ -2860,8 +2867,13 @@ cudaError_t launch_em_avg(Fields in, Fields out, int N, const EmArgs &a, double 
                           double *avg_out, cudaStream_t st) {
   const Geo g = make_geo(N);
   const unsigned nb = nblocks(g.V2, kThreads);
-  if (a.xi) em_kernel<true, true><<<nb, kThreads, 0, st>>>(in, out, g, a, partial, done, avg_out);
-  else em_kernel<false, true><<<nb, kThreads, 0, st>>>(in, out, g, a, partial, done, avg_out);
+  if (idx32(g)) {
+    if (a.xi) em_kernel<true, true, int><<<nb, kThreads, 0, st>>>(in, out, g, a, partial, done, avg_out);
+    else em_kernel<false, true, int><<<nb, kThreads, 0, st>>>(in, out, g, a, partial, done, avg_out);
+  } else {
+    if (a.xi) em_kernel<true, true, long long><<<nb, kThreads, 0, st>>>(in, out, g, a, partial, done, avg_out);
+    else em_kernel<false, true, long long><<<nb, kThreads, 0, st>>>(in, out, g, a, partial, done, avg_out);
+  }
   return cudaGetLastError();
 }
 
