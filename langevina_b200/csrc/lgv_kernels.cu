@@ -1257,9 +1257,12 @@ __device__ __forceinline__ void em_pair(const Fields &in, const Fields &out, con
 
 // One thread per site pair (element m of both parity half rows of row (j, k)),
 // flat over the V/2 pairs.  AVG: also the volume averages of the new phi into
-// avg_out[0..3] (grid_sum4).
+// avg_out[0..3] (grid_sum4).  Six 256-thread CTAs per SM (40 registers): the
+// step is bound by issue and its loads' latency, and measured fastest there
+// (0.399 ms per 256^3 step against 0.404 at five, 0.420 at four, 0.399 at
+// seven or eight with more spill).
 template <bool INJECTED, bool AVG, typename I>
-__global__ void __launch_bounds__(kThreads, 4) em_kernel(Fields in, Fields out, Geo g, EmArgs a, double *partial,
+__global__ void __launch_bounds__(kThreads, 6) em_kernel(Fields in, Fields out, Geo g, EmArgs a, double *partial,
                                                       unsigned *done, double *avg_out) {
   const long long idx = (long long)blockIdx.x * kThreads + threadIdx.x;
   double acc[4] = {0, 0, 0, 0};
