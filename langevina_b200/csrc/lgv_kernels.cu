@@ -29,6 +29,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
+#include <mutex>
 #include <vector>
 
 namespace lgv {
@@ -3019,12 +3020,20 @@ cudaError_t launch_batch_charge(const RepDesc *d, const EnsDyn *dyn, const int *
 }
 
 int persist_grid(bool i32) {
-  static int cached[2] = {-1, -1};
-  int &c = cached[i32 ? 1 : 0];
+  // per device (the shared-memory attribute is set on the current device)
+  constexpr int kMaxDevices = 64;
+  static int cached[kMaxDevices][2];
+  static std::once_flag once;
+  std::call_once(once, [] {
+    for (auto &d : cached) d[0] = d[1] = -1;
+  });
+  int dev = 0, coop = 0, sms = 0, per = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return 0;
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lk(mu);
+  int &c = cached[dev][i32 ? 1 : 0];
   if (c >= 0) return c;
   c = 0;
-  int dev = 0, coop = 0, sms = 0, per = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
   if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop) return 0;
   if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
   const void *kern = i32 ? (const void *)ens_persistent_kernel<int> : (const void *)ens_persistent_kernel<long long>;
