@@ -109,7 +109,7 @@ class ClockSampler:
         self.f.seek(0)
         rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
         os.unlink(self.f.name)
-        mhz, mx, reasons, watts = [], None, set(), []
+        mhz, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for r in rows:
             try:
@@ -117,15 +117,11 @@ class ClockSampler:
                 mx = float(r[2].split()[0])
             except (ValueError, IndexError):
                 continue
-            try:
-                watts.append(float(r[3].split()[0]))
-            except (ValueError, IndexError):
-                pass
             for n, v in zip(names, r[5:9]):
                 if "Active" in v and "Not" not in v:
                     reasons.add(n)
         return {"sm_mhz": statistics.median(mhz) if mhz else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(mhz), "power_w": statistics.median(watts) if watts else None}
+                "samples": len(mhz)}
 
 
 def reference_build_run(N, scounts, warmup, steps, ranks, seed=122335456):
