@@ -333,8 +333,8 @@ int lgv_ensemble_synchronize(lgv_ensemble *e);
 #define LGV_NOALLOC_MAX_N 128
 int lgv_measure_aos_noalloc(const double *dev_aos, int N, double *dev_out, void *stream);
 
-/* ---- Lattices split into z-slabs over ranks (no single
- * counterpart: it replaces the z-decomposition of DMDACreate3d,
+/* ---- Lattices split into z-slabs over ranks, for lattices larger than one
+ * GPU (no single counterpart: it replaces the z-decomposition of DMDACreate3d,
  * ModelA.h:315-318, with its ghost exchanges DMGlobalToLocal before every
  * pass, Stepper.cxx:81-82, 312-315, 477-480).
  *
