@@ -34,6 +34,11 @@ int fail(int code, const char *fmt, ...) {
   vsnprintf(buf, sizeof(buf), fmt, ap);
   va_end(ap);
   g_last_error = buf;
+  // A failed runtime call (an allocation above all) leaves its error as the
+  // runtime's last error, which the next launch's cudaGetLastError would
+  // report as its own: clear it now that it is reported here.  (Sticky
+  // errors of a lost context are not cleared by this and stay visible.)
+  if (code == LGV_ERR_CUDA || code == LGV_ERR_NOMEM) (void)cudaGetLastError();
   return code;
 }
 

@@ -35,6 +35,9 @@ namespace {
 
 int efail(int code, const std::string &msg) {
   lgv_internal_set_error(msg.c_str());
+  // as fail() in lgv_capi.cu: the reported runtime error must not surface
+  // again at the next launch
+  if (code == LGV_ERR_CUDA || code == LGV_ERR_NOMEM) (void)cudaGetLastError();
   return code;
 }
 
