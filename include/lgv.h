@@ -147,6 +147,17 @@ int lgv_initialize(lgv_handle *h, int kind, double scale);
  * counter streams; saving (seed, counter) replaces the <tag>_<rank>.rng file
  * (NoiseGenerator.h:112-146). */
 int lgv_set_noise_mode(lgv_handle *h, int mode);
+/* Proposal of the phi heat bath with counter noise: LGV_HB_PROPOSAL_UNIFORM
+ * (the default: U(-sqrt3, sqrt3) per component, as EulerLangevinHB::step,
+ * Stepper.cxx:343) or LGV_HB_PROPOSAL_GAUSSIAN (four normals per site, two
+ * Box-Muller pairs from the site's first four draws; variance one as well, so
+ * the same proposal scale and detailed balance).  Injected proposals are used
+ * as given either way.  Gaussian proposals run on the one-parity pass kernel:
+ * LGV_ERR_UNSUPPORTED when LGV_HB_FUSED or LGV_HB_ORDERED was set at
+ * creation; ensembles propose uniformly. */
+#define LGV_HB_PROPOSAL_UNIFORM 0
+#define LGV_HB_PROPOSAL_GAUSSIAN 1
+int lgv_set_hb_proposal(lgv_handle *h, int kind);
 int lgv_set_counter(lgv_handle *h, uint64_t counter);
 int lgv_get_counter(lgv_handle *h, uint64_t *counter);
 /* Injected noise for the next sub-step of each kind (host pointers, copied).

@@ -24,6 +24,7 @@ PV2HBSPLIT, PV2HBSPLIT_NODIFFUSE, PV2HBSPLIT_ONLYDIFFUSE = 0, 1, 2
 IDEAL_PV2, EULER_LANGEVIN_HB, CHARGE_HB, MODELA_EM, IDEAL_EM = 3, 4, 5, 6, 7
 NOISE_COUNTER, NOISE_INJECTED = 0, 1
 INIT_ZERO, INIT_PHI_GAUSSIAN, INIT_CHARGES_GAUSSIAN = 0, 1, 2
+HB_PROPOSAL_UNIFORM, HB_PROPOSAL_GAUSSIAN = 0, 1
 MONITOR_IDEAL, MONITOR_PHI_HB, MONITOR_CHARGE_HB = 0, 1, 2
 KCLASS_IDEAL, KCLASS_PHI_HB, KCLASS_CHARGE, KCLASS_EM, KCLASS_MEASURE = 0, 1, 2, 3, 4
 PACK_GIVEN, PACK_LARGEST_FIRST, PACK_INTERLEAVED = 0, 1, 2
@@ -67,6 +68,7 @@ SIGNATURES = [
     ("lgv_get_state_device", C.c_int, [_H, C.c_void_p]),
     ("lgv_initialize", C.c_int, [_H, C.c_int, C.c_double]),
     ("lgv_set_noise_mode", C.c_int, [_H, C.c_int]),
+    ("lgv_set_hb_proposal", C.c_int, [_H, C.c_int]),
     ("lgv_set_counter", C.c_int, [_H, C.c_uint64]),
     ("lgv_get_counter", C.c_int, [_H, C.POINTER(C.c_uint64)]),
     ("lgv_inject_hb", C.c_int, [_H, C.c_void_p, C.c_void_p]),

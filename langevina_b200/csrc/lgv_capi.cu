@@ -117,6 +117,8 @@ struct lgv_handle {
   // bottom-up.
   bool zalt = true;
   int zrev = 0;
+  // Gaussian phi heat-bath proposals with counter noise (lgv_set_hb_proposal)
+  bool hb_gauss = false;
   // Geometry of the buffers: the whole lattice, or for a slab handle
   // (lgv_slab_create) its planes k0 .. k0+nz-1 with two ghost planes on each
   // side, filled by the caller's halo exchange before every sub-pass that
@@ -338,6 +340,7 @@ int sub_hb(lgv_handle *h, double dt, double mass) {  // EulerLangevinHB::step (S
     a.acc = h->inj_hb_acc;
   } else {
     a.sk = lgv::sub_key(h->key, h->ctr);
+    a.gauss = h->hb_gauss ? 1 : 0;
   }
   if (h->hb_ordered) {
     KTimer tm(h, LGV_KCLASS_PHI_HB, 2);  // one launch, both parity passes
@@ -786,6 +789,16 @@ int lgv_set_noise_mode(lgv_handle *h, int mode) {
   if (mode != LGV_NOISE_COUNTER && mode != LGV_NOISE_INJECTED) return fail(LGV_ERR_INVALID, "noise mode %d", mode);
   if (mode == LGV_NOISE_INJECTED) LGV_TRY(no_slab(h, "injected noise"));
   h->noise_mode = mode;
+  return LGV_OK;
+}
+
+int lgv_set_hb_proposal(lgv_handle *h, int kind) {
+  if (!h) return fail(LGV_ERR_INVALID, "handle is NULL");
+  if (kind != LGV_HB_PROPOSAL_UNIFORM && kind != LGV_HB_PROPOSAL_GAUSSIAN)
+    return fail(LGV_ERR_INVALID, "heat-bath proposal kind %d", kind);
+  if (kind == LGV_HB_PROPOSAL_GAUSSIAN && (h->hb_fused || h->hb_ordered))
+    return fail(LGV_ERR_UNSUPPORTED, "Gaussian proposals run on the one-parity pass only (LGV_HB_FUSED / LGV_HB_ORDERED set)");
+  h->hb_gauss = kind == LGV_HB_PROPOSAL_GAUSSIAN;
   return LGV_OK;
 }
 

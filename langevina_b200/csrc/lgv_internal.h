@@ -27,6 +27,7 @@ struct HbArgs {
   const double *acc;    // injected [V] or null
   uint8_t *flags;       // [V] or null
   MonAcc *mon;          // or null
+  int gauss;            // counter noise: Gaussian proposals (lgv_set_hb_proposal); the one-parity pass only
 };
 
 struct ChargeArgs {

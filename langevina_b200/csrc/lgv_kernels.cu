@@ -273,15 +273,26 @@ struct HbDecision {
   uint8_t flag;
 };
 
-template <bool INJECTED>
+// GAUSS (counter noise): the proposals are the four normals of two
+// Box-Muller pairs from the site's first four draws (as Euler-Maruyama's
+// noise) instead of the reference's U(-sqrt3, sqrt3), Stepper.cxx:343; both
+// are symmetric with variance one, so detailed balance and the proposal scale
+// are the same.  The accept uniform is the next draw either way.
+template <bool INJECTED, bool GAUSS = false>
 __device__ __forceinline__ void hb_decide(const double po[4], const double heff[4], const HbArgs &a, long long nat,
                                           long long V, HbDecision &r) {
   Xoro rng;
   if (!INJECTED) rng = stream_at(a.sk, (uint64_t)nat);
+  double z[4] = {0., 0., 0., 0.};
+  if (!INJECTED && GAUSS) {
+    const uint64_t r1 = rng.next(), r2 = rng.next(), r3 = rng.next(), r4 = rng.next();
+    box_muller(r1, r2, z[0], z[1]);
+    box_muller(r3, r4, z[2], z[3]);
+  }
   double hphi_o = 0., hphi_n = 0., s_o = 0., s_n = 0.;
 #pragma unroll
   for (int l = 0; l < 4; ++l) {
-    const double v = INJECTED ? a.prop[(long long)l * V + nat] : var1(rng.next());
+    const double v = INJECTED ? a.prop[(long long)l * V + nat] : (GAUSS ? z[l] : var1(rng.next()));
     r.pn[l] = po[l] + a.rdtg * v;
     s_o += po[l] * po[l];
     s_n += r.pn[l] * r.pn[l];
@@ -336,7 +347,7 @@ __device__ __forceinline__ I nat_index_t(const Geo &g, int i, int j, int k) {
   return ((I)kk * g.N + j) * g.N + i;
 }
 
-template <bool INJECTED, bool MON, bool CG = false, typename I = long long>
+template <bool INJECTED, bool MON, bool CG = false, typename I = long long, bool GAUSS = false>
 __device__ __forceinline__ void hb_site(const Fields &f, const Geo &g, int parity, const HbArgs &a, int m, int j,
                                         int k, MonLocal &mon) {
   const int H = g.H, N = g.N;
@@ -363,7 +374,7 @@ __device__ __forceinline__ void hb_site(const Fields &f, const Geo &g, int parit
   }
   const long long nat = (long long)nat_index_t<I>(g, 2 * m + s, j, k);
   HbDecision d;
-  hb_decide<INJECTED>(po, heff, a, nat, global_sites(g), d);
+  hb_decide<INJECTED, GAUSS>(po, heff, a, nat, global_sites(g), d);
   if (d.accept) {
 #pragma unroll
     for (int l = 0; l < 4; ++l) f.c[l][own] = d.pn[l];
@@ -397,11 +408,11 @@ __host__ __forceinline__ dim3 pass_grid(const Geo &g, bool rows) {
   return rows ? dim3(g.H / 128, g.N, g.Nz) : dim3((unsigned)(((long long)g.N * g.H + 127) / 128), g.Nz);
 }
 
-template <bool INJECTED, bool MON, bool ROWS, typename I>
+template <bool INJECTED, bool MON, bool ROWS, typename I, bool GAUSS = false>
 __global__ void __launch_bounds__(128) hb_pass_kernel(Fields f, Geo g, int parity, HbArgs a) {
   int m, j, k;
   MonLocal mon;
-  if (pass_site<ROWS>(g, m, j, k)) hb_site<INJECTED, MON, false, I>(f, g, parity, a, m, j, k, mon);
+  if (pass_site<ROWS>(g, m, j, k)) hb_site<INJECTED, MON, false, I, GAUSS>(f, g, parity, a, m, j, k, mon);
   if (MON) mon_flush(mon, a.mon);
 }
 
@@ -2569,18 +2580,20 @@ cudaError_t launch_hb_pass(Fields f, int N, int parity, const HbArgs &a, cudaStr
 }
 
 cudaError_t launch_hb_pass(Fields f, const Geo &g, int parity, const HbArgs &a, cudaStream_t st) {
-  if (g.Nz == g.Ng && g.kg == 0 && hb_zpass_default(g.N)) return launch_hb_zpass(f, g.N, parity, a, st);
+  const bool inj = a.prop != nullptr, mon = a.mon != nullptr;
+  const bool gauss = a.gauss && !inj;  // injected proposals are used as given
+  if (!gauss && g.Nz == g.Ng && g.kg == 0 && hb_zpass_default(g.N)) return launch_hb_zpass(f, g.N, parity, a, st);
   const bool rows = g.H % 128 == 0;
   const dim3 grid = pass_grid(g, rows);
-  const bool inj = a.prop != nullptr, mon = a.mon != nullptr;
   const bool i32 = idx32(g);
-#define LGV_HBP1(I, M, T)                                                                                    \
-  if (rows) hb_pass_kernel<I, M, true, T><<<grid, 128, 0, st>>>(f, g, parity, a);                           \
-  else hb_pass_kernel<I, M, false, T><<<grid, 128, 0, st>>>(f, g, parity, a)
-#define LGV_HBP(I, M)                                                                                        \
-  if (i32) { LGV_HBP1(I, M, int); } else { LGV_HBP1(I, M, long long); }
-  if (inj) { if (mon) { LGV_HBP(true, true); } else { LGV_HBP(true, false); } }
-  else { if (mon) { LGV_HBP(false, true); } else { LGV_HBP(false, false); } }
+#define LGV_HBP1(I, M, T, G)                                                                                 \
+  if (rows) hb_pass_kernel<I, M, true, T, G><<<grid, 128, 0, st>>>(f, g, parity, a);                        \
+  else hb_pass_kernel<I, M, false, T, G><<<grid, 128, 0, st>>>(f, g, parity, a)
+#define LGV_HBP(I, M, G)                                                                                     \
+  if (i32) { LGV_HBP1(I, M, int, G); } else { LGV_HBP1(I, M, long long, G); }
+  if (inj) { if (mon) { LGV_HBP(true, true, false); } else { LGV_HBP(true, false, false); } }
+  else if (gauss) { if (mon) { LGV_HBP(false, true, true); } else { LGV_HBP(false, false, true); } }
+  else { if (mon) { LGV_HBP(false, true, false); } else { LGV_HBP(false, false, false); } }
 #undef LGV_HBP
 #undef LGV_HBP1
   return cudaGetLastError();

@@ -194,6 +194,10 @@ struct Handle {
   std::vector<std::array<lgv_monitor, 3>> mon;
   bool flags_on = false;
   std::vector<uint8_t> flags;
+  // counter noise only: Gaussian phi heat-bath proposals (the four normals of
+  // two Box-Muller pairs from the site's first four draws) instead of the
+  // reference's U(-sqrt3, sqrt3); lgv_set_hb_proposal of the CUDA library
+  bool hb_gauss = false;
   double last_E[2] = {0, 0};
   std::vector<double> part;  // per-rank scratch for reductions
 
@@ -369,13 +373,18 @@ static void hb_sweep(Handle &h, double dt, double mass) {
             const double *zp = S + h.idx(i, j, k + 1) * LGV_NDOF, *zm = S + h.idx(i, j, k - 1) * LGV_NDOF;
             CtrStream cs(sk, h.mode == CTR ? n : 0);
             double hphi_o = 0., hphi_n = 0., s_o = 0., s_n = 0.;
-            double pn[4];
+            double pn[4], z[4] = {0, 0, 0, 0};
+            if (h.mode == CTR && h.hb_gauss) {
+              const uint64_t r1 = cs.next(), r2 = cs.next(), r3 = cs.next(), r4 = cs.next();
+              box_muller(r1, r2, z[0], z[1]);
+              box_muller(r3, r4, z[2], z[3]);
+            }
             for (int l = 0; l < 4; ++l) {
               const double heff = (xp[l] + xm[l]) + (yp[l] + ym[l]) + (zp[l] + zm[l]);
               const double po = c[l];
               double v;
               if (h.mode == SEQ) v = g.variance1();
-              else if (h.mode == CTR) v = v1_of(cs.next());
+              else if (h.mode == CTR) v = h.hb_gauss ? z[l] : v1_of(cs.next());
               else v = h.hb_prop[(size_t)l * h.V + n];
               pn[l] = po + rdtg * v;
               s_o += std::pow(po, 2);
@@ -940,6 +949,8 @@ void orc_get_monitor(void *hh, int which, lgv_monitor *out) {
   }
   *out = m;
 }
+
+void orc_set_hb_proposal(void *hh, int kind) { ((Handle *)hh)->hb_gauss = kind == 1; }
 
 void orc_debug_flags(void *hh, int on) {
   Handle *h = (Handle *)hh;

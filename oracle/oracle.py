@@ -60,6 +60,7 @@ def load():
         "orc_last_energies": (None, [V, C.c_void_p]),
         "orc_get_monitor": (None, [V, C.c_int, C.c_void_p]),
         "orc_debug_flags": (None, [V, C.c_int]),
+        "orc_set_hb_proposal": (None, [V, C.c_int]),
         "orc_get_flags": (None, [V, C.c_void_p]),
         "orc_o4_rotation": (None, [C.c_void_p, C.c_void_p, C.c_void_p]),
         "orc_seq_draws": (None, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]),
@@ -128,15 +129,24 @@ class Oracle:
     def get_counter(self):
         return int(self.lib.orc_get_counter(self.h))
 
+    # (the contiguous copies are held in locals while the library reads them)
     def inject_hb(self, prop, acc):
-        self.lib.orc_inject_hb(self.h, _ptr(np.ascontiguousarray(prop)), _ptr(np.ascontiguousarray(acc)))
+        prop, acc = np.ascontiguousarray(prop), np.ascontiguousarray(acc)
+        self.lib.orc_inject_hb(self.h, _ptr(prop), _ptr(acc))
 
     def inject_charge(self, order, q, acc):
         o = np.ascontiguousarray(order, dtype=np.int32)
-        self.lib.orc_inject_charge(self.h, _ptr(o), _ptr(np.ascontiguousarray(q)), _ptr(np.ascontiguousarray(acc)))
+        q, acc = np.ascontiguousarray(q), np.ascontiguousarray(acc)
+        self.lib.orc_inject_charge(self.h, _ptr(o), _ptr(q), _ptr(acc))
 
     def inject_em(self, xi):
-        self.lib.orc_inject_em(self.h, _ptr(np.ascontiguousarray(xi)))
+        xi = np.ascontiguousarray(xi)
+        self.lib.orc_inject_em(self.h, _ptr(xi))
+
+    def set_hb_proposal(self, kind):
+        """0: uniform U(-sqrt3, sqrt3) proposals (the reference's); 1: Gaussian
+        (counter noise only, as the CUDA library's lgv_set_hb_proposal)."""
+        self.lib.orc_set_hb_proposal(self.h, int(kind))
 
     def step(self, evolver, dt, t=0.0, nsteps=1, inner=1, outer=1):
         rc = self.lib.orc_step(self.h, evolver, inner, outer, float(dt), float(t), int(nsteps))
