@@ -454,6 +454,11 @@ class ModelA {
     return u;
   }
   void set_state(const std::vector<double> &u) { check(lgv_set_state(handle, u.data()), "lgv_set_state"); }
+  // Gaussian phi heat-bath proposals instead of the reference's uniform ones
+  void set_hb_proposal(bool gaussian) {
+    check(lgv_set_hb_proposal(handle, gaussian ? LGV_HB_PROPOSAL_GAUSSIAN : LGV_HB_PROPOSAL_UNIFORM),
+          "lgv_set_hb_proposal");
+  }
 
   // <tag>_save.npy: shape (NZ, NY, NX, 10), the o4fields layout
   void write(const std::string &tag) const {

@@ -157,6 +157,12 @@ class ModelA:
     def set_counter(self, c):
         L.check(self.lib.lgv_set_counter(self.handle, int(c)), "lgv_set_counter")
 
+    def set_hb_proposal(self, gaussian):
+        """Gaussian phi heat-bath proposals (True) or the reference's uniform
+        U(-sqrt3, sqrt3) ones (False, the default); lgv_set_hb_proposal."""
+        kind = L.HB_PROPOSAL_GAUSSIAN if gaussian else L.HB_PROPOSAL_UNIFORM
+        L.check(self.lib.lgv_set_hb_proposal(self.handle, kind), "lgv_set_hb_proposal")
+
     def get_counter(self):
         c = C.c_uint64()
         L.check(self.lib.lgv_get_counter(self.handle, C.byref(c)), "lgv_get_counter")
