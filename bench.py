@@ -209,14 +209,19 @@ def run_reference(a):
               "N": a.N, "evolver": name, "dt": DT, **COEF}
     if reference_available():
         R = max(1, min(cores, a.N // 2))
-        rate, ms, el = reference_build_run(a.N, scounts, a.warmup, a.steps, R)
+        # a reference step of the 256^3 lattice takes ~3 s on 16 cores: at most
+        # REF_MAX_STEPS timed steps (and 3 warm-up) keep the run within minutes
+        nst, nw = min(a.steps, REF_MAX_STEPS), min(a.warmup, 3)
+        rate, ms, el = reference_build_run(a.N, scounts, nw, nst, R)
         cpu = {"kind": "reference", "cores": R,
-               "sample": f"the whole workload: {a.steps} timed steps after {a.warmup} warm-up on the {a.N}^3 "
-                         f"lattice ({el:.1f} s), the reference's Stepper.cxx/NoiseGenerator.cxx/measurer.cxx built "
-                         f"unmodified against single-node PETSc/MPI/FFTW stand-ins, {R} MPI ranks (processes)"}
+               "sample": f"the whole workload, {nst} timed steps after {nw} warm-up on the {a.N}^3 lattice "
+                         f"({el:.1f} s; at most {REF_MAX_STEPS} timed steps whatever --steps asks), the reference's "
+                         f"Stepper.cxx/NoiseGenerator.cxx/measurer.cxx built unmodified against single-node "
+                         f"PETSc/MPI/FFTW stand-ins, {R} MPI ranks (processes)"}
         config["implementation"] = "reference stepper and measurer (oracle/_ref/ref_stepper)"
     else:
         Ns = min(a.N, 128)
+        nst, nw = a.steps, a.warmup
         rate, ms, el, R = cpu_port_rate(Ns, scounts, a.steps, a.warmup)
         cpu = {"kind": "port", "cores": R,
                "sample": f"{a.steps} timed steps of a {Ns}^3 sample lattice ({el:.1f} s), oracle port with the "
@@ -225,7 +230,7 @@ def run_reference(a):
     cpu.update(value=rate, unit="site-updates/s")
     line = {
         "impl": "reference", "metric": "Model G site-updates/s", "value": rate, "unit": "site-updates/s",
-        "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms,
+        "n_gpus": a.gpus, "steps": nst, "warmup": nw, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": config, "cpu_baseline": cpu,
         "e2e": {"value": rate, "unit": "site-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -234,6 +239,7 @@ def run_reference(a):
     return 0
 
 
+REF_MAX_STEPS = 30  # timed steps of the reference arm at most (bench.py --impl reference)
 ENSEMBLE = [(32, 256), (48, 64), (64, 16)]  # (N, replicas)
 ENS_H = (0.003, 0.006, 0.012)
 
